@@ -1,0 +1,113 @@
+"""ctypes binding of libhelixrecon.so (the C ABI declared in include/helixrecon.h).
+
+There is no fallback: if the library is missing or cannot be loaded, every
+call raises. Device pointers are passed as integers (e.g. ``tensor.data_ptr()``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libhelixrecon.so")
+
+HR_OK = 0
+HR_FORM_PLAIN, HR_FORM_FP64, HR_FORM_FAST = 0, 1, 2
+HR_LAYOUT_ROWS, HR_LAYOUT_REBIN = 0, 1
+
+_i = ctypes.c_int
+_f = ctypes.c_float
+_d = ctypes.c_double
+_p = ctypes.c_void_p
+
+
+class HelixError(RuntimeError):
+    """A library call returned a non-zero hr_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"helixrecon status {status}: {message}")
+        self.status = status
+
+
+class BpGeom(ctypes.Structure):
+    _fields_ = ([(n, _i) for n in ("N_2pi", "XN", "YN", "ZN", "YL", "ZL", "PN")]
+                + [(n, _d) for n in ("XNC", "YNC", "ZNC", "dx", "dy", "dz", "YLC", "ZLC", "dYL", "dZL", "h", "BetaS",
+                                     "DeltaFai", "N_pi", "HSCoef", "SO", "SD", "k1")])
+
+    @classmethod
+    def from_dict(cls, g: dict) -> "BpGeom":
+        return cls(**{k: g[k] for k, _ in cls._fields_})
+
+
+class ReconDesc(ctypes.Structure):
+    _fields_ = ([("YL", _i), ("ZL", _i), ("ViewN", _i)]
+                + [(n, _f) for n in ("YLC", "dYA", "DeltaTheta", "PLC", "DeltaT", "DeltaFai", "SO")]
+                + [("view0", _i)] + [(n, _f) for n in ("fPLC", "fZLC", "fdYL", "fdZL", "fSO")]
+                + [("bp", BpGeom), ("w", _p), ("form", _i)])
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "hr_last_error": (ctypes.c_char_p, []),
+    "hr_version": (_i, []),
+    "hr_view_weights": (_i, [_p, _i, _d, _i]),
+    "ParallelRebinningCBCurve_GPU": (None, [_p, _p, _i, _i, _i] + [_f] * 7),
+    "filtering": (None, [_p, _p, _i, _i, _i] + [_f] * 5),
+    "ParallekFDKHelical3DWeighting_GPU_float": (None, [_p, _p, _p, _i, _i, _i, _i] + [_f] * 6 + [_i] * 3 + [_f] * 12),
+    "ParallekFDKHelical3DWeighting_GPU_double": (None, [_p, _p, _p, _i, _i, _i, _i] + [_d] * 6 + [_i] * 3 + [_d] * 12),
+    "ParallelFDKHelical3DWeighting": (None, [_p, _p, _d, _d, _i, _i] + [_d] * 6 + [_i, _i, _d, _i, _i, _i] + [_d] * 3
+                                      + [_i, _d, _d, _i]),
+    "hr_rebin_host": (_i, [_p, _p, _i, _i, _i] + [_f] * 7),
+    "hr_filter_host": (_i, [_p, _p, _i, _i, _i] + [_f] * 5),
+    "hr_bp_host_float": (_i, [_p, _p, _p, _i, _i, _i, _i] + [_f] * 6 + [_i] * 3 + [_f] * 12),
+    "hr_bp_host_double": (_i, [_p, _p, _p, _i, _i, _i, _i] + [_d] * 6 + [_i] * 3 + [_d] * 12),
+    "hr_bp_host_reference": (_i, [_p, _p, _d, _d, _i, _i] + [_d] * 6 + [_i, _i, _d, _i, _i, _i] + [_d] * 3
+                             + [_i, _d, _d, _i]),
+    "hr_rebin_plan_create": (_i, [ctypes.POINTER(_p), _i, _i, _i] + [_f] * 7),
+    "hr_rebin_execute": (_i, [_p, _p, _p, _p]),
+    "hr_rebin_plan_destroy": (None, [_p]),
+    "hr_filter_plan_create": (_i, [ctypes.POINTER(_p), _i, _i, _i] + [_f] * 5),
+    "hr_filter_execute": (_i, [_p, _p, _p, _i, _i, _p]),
+    "hr_filter_plan_destroy": (None, [_p]),
+    "hr_bp_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(BpGeom), _p, _i]),
+    "hr_bp_execute": (_i, [_p, _p, _p, _p]),
+    "hr_bp_plan_destroy": (None, [_p]),
+    "hr_project_ellipsoids": (_i, [_p, _i, _i, _i] + [_d] * 9 + [_p, _i, _p]),
+    "hr_recon_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc)]),
+    "hr_recon_execute": (_i, [_p, _p, _p, _p]),
+    "hr_recon_execute_host": (_i, [_p, _p, _p]),
+    "hr_recon_device_bytes": (ctypes.c_size_t, [_p]),
+    "hr_recon_plan_destroy": (None, [_p]),
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the library (once). Raises if it is missing: there is no CPU path."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `python -m analyticalreconbigpatient_b200.build`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def check(status: int) -> None:
+    if status != HR_OK:
+        msg = load().hr_last_error()
+        raise HelixError(status, msg.decode() if msg else "")
+
+
+def call(name: str, *args):
+    """Call a status-returning entry and raise HelixError on failure."""
+    check(getattr(load(), name)(*args))

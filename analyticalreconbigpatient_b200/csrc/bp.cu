@@ -1,0 +1,343 @@
+// 3D-weighted helical parallel-cone backprojection (plain FP32 and FP64 forms).
+//
+// Reference: src/Parallel_FDK_Helical_3DWeighting.cpp:42-113 (CPU, the parity
+// target) and src/ParallelFDKHelical3DWeightingGPU.cu:14-87 (GPU). For voxel
+// (x, y, z): s0 = ceil((2 pi z/h - BetaS)/DeltaFai - 0.5), views
+// s0 -/+ ceil(N_pi HSCoef) clamped to [0, PN-1] (the CPU loop; the reference
+// GPU loop starts at view 0 and reads w[] out of bounds for far views), and
+// per view: UU, Yr, temp1 = sqrt(SO^2 - Yr^2), temp2 = z - h View/2pi,
+// Zr = temp2 SO SD/(UU temp1 + SO^2 - Yr^2), U = ceil(Yr/dYL + YLC),
+// V = ceil(Zr/dZL + ZLC), bilinear tap if 0 < U < YL and 0 < V < ZL, and the
+// 3D weight w[d1] Gama_C^k1 / (w[d2] Gama^k1 + w[d1] Gama_C^k1).
+//
+// Index selection is bit-exact to the CPU path: x, y, z, s0, UU, Yr, temp1,
+// U1 and temp2 are evaluated in double with the reference's operation order
+// through non-contracting __d*_rn intrinsics, from per-view cos/sin/h*View/2pi
+// tables that the plan computes on the host with the same C library calls. V
+// is first located with one FMA from a per-(column, view) slope; only when
+// that estimate lies within 1e-9 of an integer (the estimate's error is below
+// 1e-12) is Zr/dZL + ZLC recomputed exactly, so ceil() never disagrees.
+//
+// Work decomposition: a thread owns NZ consecutive voxels of one (x, y)
+// column. Everything that does not depend on z (the trig, UU, Yr, temp1, U,
+// Dey, the projection slope, 1/(temp1 +- UU)) is computed once per column and
+// view and reused for the NZ voxels; the NZ windows [s1, s2] are uniform over
+// the CTA (all its threads share the z block), so the per-voxel window test
+// is a uniform branch. A warp is an 8 x 4 (x, y) tile, which keeps its 32
+// detector taps within a few cache lines of one or two rows.
+#include <cmath>
+#include <vector>
+
+#include "hr_internal.h"
+
+namespace {
+
+constexpr int kBx = 8, kBy = 16;  // CTA tile (x, y); warps are 8 x 4
+constexpr double kTwoPiTrunc = 2.0 * 3.14159265358979;         // ..._3DWeighting.cpp:16,62
+constexpr double kInvTwoPi = 1.0 / (2.0 * 3.141592653589793);  // :51,79
+
+struct ViewTab {
+  double c, s, hv;  // cos(View), sin(View), h*View*invPI
+};
+
+struct BpParams {
+  int XN, YN, ZN, YL, ZL, PN, N_2pi, half;
+  double XNC, YNC, ZNC, dx, dy, dz, YLC, ZLC, dYL, dZL, h, BetaS, DeltaFai, N_pi, SO, SD, k1;
+  double SO2, SOSD, SOSDdZL;
+  float k1f, DeltaFaif;
+};
+
+}  // namespace
+
+struct hr_bp_plan {
+  BpParams prm;
+  int form;
+  ViewTab* d_views;
+  float* d_w;
+  double* d_wd;
+};
+
+namespace {
+
+// Voxel centre and central view, exactly as the CPU reference.
+struct ZInfo {
+  double z;
+  int s0, lo, hi;
+};
+
+__device__ __forceinline__ ZInfo z_info(const BpParams& P, int zi) {
+  ZInfo r;
+  r.z = __dmul_rn(__dsub_rn((double)zi, P.ZNC), P.dz);
+  const double beta0 = __ddiv_rn(__dmul_rn(kTwoPiTrunc, r.z), P.h);
+  const double sarg = __dsub_rn(__ddiv_rn(__dsub_rn(beta0, P.BetaS), P.DeltaFai), 0.5);
+  r.s0 = (int)ceil(sarg);
+  const int s1 = r.s0 - P.half, s2 = r.s0 + P.half;
+  if (zi < P.ZN && s1 < P.PN && s2 > 0) {
+    r.lo = s1 < 0 ? 0 : s1;
+    r.hi = s2 > P.PN - 1 ? P.PN - 1 : s2;
+  } else {
+    r.lo = 0x7fffffff;
+    r.hi = -0x7fffffff;
+  }
+  return r;
+}
+
+// Per (column, view) quantities.
+struct ColView {
+  int U;          // channel of the upper tap
+  double U1;      // Yr/dYL + YLC
+  double denom;   // UU*temp1 + SO^2 - Yr^2
+  double A, B;    // temp1 + UU, temp1 - UU
+  double slope;   // SO SD / dZL / denom
+};
+
+__device__ __forceinline__ ColView col_view(const BpParams& P, double x, double y, const ViewTab& v) {
+  ColView r;
+  const double UU = __dsub_rn(__dmul_rn(-x, v.c), __dmul_rn(y, v.s));
+  const double Yr = __dadd_rn(__dmul_rn(-x, v.s), __dmul_rn(y, v.c));
+  const double Yr2 = __dmul_rn(Yr, Yr);
+  const double temp1 = __dsqrt_rn(__dsub_rn(P.SO2, Yr2));
+  r.denom = __dsub_rn(__dadd_rn(__dmul_rn(UU, temp1), P.SO2), Yr2);
+  r.U1 = __dadd_rn(__ddiv_rn(Yr, P.dYL), P.YLC);
+  r.U = (int)ceil(r.U1);
+  r.A = __dadd_rn(temp1, UU);
+  r.B = __dsub_rn(temp1, UU);
+  r.slope = P.SOSDdZL / r.denom;
+  return r;
+}
+
+// Row index V and its fraction Dez = V - V1, bit-exact to the reference.
+__device__ __forceinline__ int row_index(const BpParams& P, const ColView& cv, double temp2, double& dez) {
+  const double v1a = fma(temp2, cv.slope, P.ZLC);
+  int V = (int)ceil(v1a);
+  double d = (double)V - v1a;
+  if (d < 1e-9 || d > 1.0 - 1e-9) {
+    const double Zr = __ddiv_rn(__dmul_rn(temp2, P.SOSD), cv.denom);
+    const double V1 = __dadd_rn(__ddiv_rn(Zr, P.dZL), P.ZLC);
+    V = (int)ceil(V1);
+    d = __dsub_rn((double)V, V1);
+  }
+  dez = d;
+  return V;
+}
+
+// ---------------------------------------------------------------------------
+// Plain form: FP32 filtered data, FP32 weights and accumulation.
+// ---------------------------------------------------------------------------
+template <int NZ>
+__global__ void __launch_bounds__(kBx* kBy) bp_plain_kernel(float* __restrict__ vol, const float* __restrict__ fp,
+                                                           const ViewTab* __restrict__ views,
+                                                           const float* __restrict__ gw, BpParams P) {
+  extern __shared__ float w_s[];  // [N_2pi]
+  for (int t = threadIdx.y * kBx + threadIdx.x; t < P.N_2pi; t += kBx * kBy) w_s[t] = gw[t];
+  __syncthreads();
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  const int z0 = blockIdx.z * NZ;
+  if (xi >= P.XN || yi >= P.YN) return;
+  const double x = __dmul_rn(__dsub_rn((double)xi, P.XNC), P.dx);
+  const double y = __dmul_rn(__dsub_rn((double)yi, P.YNC), P.dy);
+  ZInfo zin[NZ];
+  float res[NZ];
+  int pstart = 0x7fffffff, pend = -0x7fffffff;
+#pragma unroll
+  for (int m = 0; m < NZ; ++m) {
+    zin[m] = z_info(P, z0 + m);
+    res[m] = 0.0f;
+    pstart = min(pstart, zin[m].lo);
+    pend = max(pend, zin[m].hi);
+  }
+  const size_t plane = (size_t)P.ZL * P.YL;
+  for (int p = pstart; p <= pend; ++p) {
+    const ViewTab v = views[p];
+    const ColView cv = col_view(P, x, y, v);
+    if (cv.U <= 0 || cv.U >= P.YL) continue;
+    const float dey = (float)((double)cv.U - cv.U1);
+    const float invA = 1.0f / (float)cv.A, invB = 1.0f / (float)cv.B;
+    const float* col = fp + (size_t)p * plane + (cv.U - 1);
+#pragma unroll
+    for (int m = 0; m < NZ; ++m) {
+      if (p < zin[m].lo || p > zin[m].hi) continue;
+      const double temp2 = __dsub_rn(zin[m].z, v.hv);
+      double dezd;
+      const int V = row_index(P, cv, temp2, dezd);
+      if (V <= 0 || V >= P.ZL) continue;
+      const float dez = (float)dezd;
+      const float* r0 = col + (size_t)(V - 1) * P.YL;
+      const float* r1 = r0 + P.YL;
+      const float ra = dey * __ldg(r0) + (1.0f - dey) * __ldg(r0 + 1);
+      const float rb = dey * __ldg(r1) + (1.0f - dey) * __ldg(r1 + 1);
+      const float touying = dez * ra + (1.0f - dez) * rb;
+      const int before = p < zin[m].s0;
+      const int d1 = (int)(P.N_pi - (double)(zin[m].s0 - p));
+      const int d2 = before ? (int)(d1 + P.N_pi) : (int)(d1 - P.N_pi);
+      const float w1 = w_s[d1], w2 = w_s[d2];
+      const float t2 = (float)temp2;
+      const float gama = fabsf(t2) * invA;
+      const float gamac = fabsf(before ? t2 - 0.5f : t2 + 0.5f) * invB;
+      const float e = exp2f(P.k1f * (log2f(gama) - log2f(gamac)));
+      const float weight = w1 / (w1 + w2 * fminf(e, 3.0e38f));
+      res[m] += weight * touying;
+    }
+  }
+  float* out = vol + ((size_t)yi * P.XN + xi) * P.ZN + z0;
+#pragma unroll
+  for (int m = 0; m < NZ; ++m)
+    if (z0 + m < P.ZN) out[m] = res[m] * P.DeltaFaif;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 form: the reference CPU's data path in double on the GPU.
+// ---------------------------------------------------------------------------
+template <int NZ>
+__global__ void __launch_bounds__(kBx* kBy) bp_fp64_kernel(double* __restrict__ vol, const double* __restrict__ fp,
+                                                          const ViewTab* __restrict__ views,
+                                                          const double* __restrict__ gw, BpParams P) {
+  extern __shared__ double wd_s[];  // [N_2pi]
+  for (int t = threadIdx.y * kBx + threadIdx.x; t < P.N_2pi; t += kBx * kBy) wd_s[t] = gw[t];
+  __syncthreads();
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  const int z0 = blockIdx.z * NZ;
+  if (xi >= P.XN || yi >= P.YN) return;
+  const double x = __dmul_rn(__dsub_rn((double)xi, P.XNC), P.dx);
+  const double y = __dmul_rn(__dsub_rn((double)yi, P.YNC), P.dy);
+  ZInfo zin[NZ];
+  double res[NZ];
+  int pstart = 0x7fffffff, pend = -0x7fffffff;
+#pragma unroll
+  for (int m = 0; m < NZ; ++m) {
+    zin[m] = z_info(P, z0 + m);
+    res[m] = 0.0;
+    pstart = min(pstart, zin[m].lo);
+    pend = max(pend, zin[m].hi);
+  }
+  const size_t plane = (size_t)P.ZL * P.YL;
+  for (int p = pstart; p <= pend; ++p) {
+    const ViewTab v = views[p];
+    const ColView cv = col_view(P, x, y, v);
+    if (cv.U <= 0 || cv.U >= P.YL) continue;
+    const double dey = __dsub_rn((double)cv.U, cv.U1);
+    const double* col = fp + (size_t)p * plane + (cv.U - 1);
+#pragma unroll
+    for (int m = 0; m < NZ; ++m) {
+      if (p < zin[m].lo || p > zin[m].hi) continue;
+      const double temp2 = __dsub_rn(zin[m].z, v.hv);
+      const double Zr = __ddiv_rn(__dmul_rn(temp2, P.SOSD), cv.denom);
+      const double V1 = __dadd_rn(__ddiv_rn(Zr, P.dZL), P.ZLC);
+      const int V = (int)ceil(V1);
+      if (V <= 0 || V >= P.ZL) continue;
+      const double dez = __dsub_rn((double)V, V1);
+      const double* r0 = col + (size_t)(V - 1) * P.YL;
+      const double* r1 = r0 + P.YL;
+      const double touying = dey * dez * r0[0] + dey * (1.0 - dez) * r1[0] + (1.0 - dey) * dez * r0[1] +
+                             (1.0 - dey) * (1.0 - dez) * r1[1];
+      const int before = p < zin[m].s0;
+      const int d1 = (int)(P.N_pi - (double)(zin[m].s0 - p));
+      const int d2 = before ? (int)(d1 + P.N_pi) : (int)(d1 - P.N_pi);
+      const double w1 = wd_s[d1], w2 = wd_s[d2];
+      const double gama = fabs(temp2 / cv.A);
+      const double gamac = before ? fabs((temp2 - 0.5) / cv.B) : fabs((temp2 + 0.5) / cv.B);
+      const double m1 = pow(gama, P.k1);
+      const double m2 = pow(gamac, P.k1);
+      const double weight = (w1 * m2) / (w2 * m1 + w1 * m2);
+      res[m] += weight * touying * P.DeltaFai;
+    }
+  }
+  double* out = vol + ((size_t)yi * P.XN + xi) * P.ZN + z0;
+#pragma unroll
+  for (int m = 0; m < NZ; ++m)
+    if (z0 + m < P.ZN) out[m] = res[m];
+}
+
+constexpr int kNzPlain = 8;
+constexpr int kNzFp64 = 4;
+
+}  // namespace
+
+extern "C" int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const double* w, int form) {
+  hr::clear_error();
+  HR_REQUIRE(plan != nullptr && g != nullptr && w != nullptr, "hr_bp_plan_create: NULL argument");
+  *plan = nullptr;
+  HR_REQUIRE(form == HR_FORM_PLAIN || form == HR_FORM_FP64, "hr_bp_plan_create: form %d not handled here", form);
+  HR_REQUIRE(g->XN > 0 && g->YN > 0 && g->ZN > 0 && g->YL > 1 && g->ZL > 1 && g->PN > 0 && g->N_2pi > 1,
+             "backprojection: invalid sizes");
+  HR_REQUIRE(g->h != 0.0 && g->DeltaFai != 0.0 && g->dYL != 0.0 && g->dZL != 0.0 && g->SO > 0.0,
+             "backprojection: h, DeltaFai, dYL, dZL must be non-zero and SO > 0");
+  HR_REQUIRE((long long)g->XN * g->YN * g->ZN < (1LL << 40), "backprojection: volume too large");
+  HR_REQUIRE(g->N_2pi <= 8192, "backprojection: N_2pi=%d exceeds 8192", g->N_2pi);
+  // For views in [s0-half, s0+half] the weight indices are d1 = N_pi-(s0-p)
+  // and d1 +/- N_pi; they stay inside [0, N_2pi) iff half <= N_pi and
+  // N_pi + half <= N_2pi - 1 (the reference GPU kernel reads outside it).
+  const int half = (int)std::ceil(g->N_pi * g->HSCoef);
+  HR_REQUIRE(half >= 0 && (double)half <= g->N_pi && g->N_pi + half <= g->N_2pi - 1 &&
+                 2.0 * g->N_pi <= g->N_2pi + 1e-9,
+             "backprojection: HSCoef=%g, N_pi=%g give a view window outside the weight table", g->HSCoef, g->N_pi);
+  HR_TRY(hr::require_device());
+
+  BpParams P{};
+  P.XN = g->XN; P.YN = g->YN; P.ZN = g->ZN; P.YL = g->YL; P.ZL = g->ZL; P.PN = g->PN; P.N_2pi = g->N_2pi;
+  P.half = half;
+  P.XNC = g->XNC; P.YNC = g->YNC; P.ZNC = g->ZNC; P.dx = g->dx; P.dy = g->dy; P.dz = g->dz;
+  P.YLC = g->YLC; P.ZLC = g->ZLC; P.dYL = g->dYL; P.dZL = g->dZL; P.h = g->h; P.BetaS = g->BetaS;
+  P.DeltaFai = g->DeltaFai; P.N_pi = g->N_pi; P.SO = g->SO; P.SD = g->SD; P.k1 = g->k1;
+  P.SO2 = g->SO * g->SO;
+  P.SOSD = g->SO * g->SD;
+  P.SOSDdZL = P.SOSD / g->dZL;
+  P.k1f = (float)g->k1;
+  P.DeltaFaif = (float)g->DeltaFai;
+
+  // Per-view tables in the reference's own arithmetic (:73, :76-79).
+  std::vector<ViewTab> tab(g->PN);
+  for (int p = 0; p < g->PN; ++p) {
+    const double View = g->BetaS + p * g->DeltaFai;
+    tab[p] = ViewTab{std::cos(View), std::sin(View), g->h * View * kInvTwoPi};
+  }
+  std::vector<float> wf(g->N_2pi);
+  for (int i = 0; i < g->N_2pi; ++i) wf[i] = (float)w[i];
+
+  hr_bp_plan* pl = new hr_bp_plan{P, form, nullptr, nullptr, nullptr};
+  cudaError_t e = cudaMalloc(&pl->d_views, sizeof(ViewTab) * g->PN);
+  if (e == cudaSuccess) e = cudaMalloc(&pl->d_w, sizeof(float) * g->N_2pi);
+  if (e == cudaSuccess) e = cudaMalloc(&pl->d_wd, sizeof(double) * g->N_2pi);
+  if (e == cudaSuccess) e = cudaMemcpy(pl->d_views, tab.data(), sizeof(ViewTab) * g->PN, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(pl->d_w, wf.data(), sizeof(float) * g->N_2pi, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(pl->d_wd, w, sizeof(double) * g->N_2pi, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(pl->d_views);
+    cudaFree(pl->d_w);
+    cudaFree(pl->d_wd);
+    delete pl;
+    return hr::fail(e == cudaErrorMemoryAllocation ? HR_ERR_OUT_OF_MEMORY : HR_ERR_CUDA, "bp plan: %s",
+                    cudaGetErrorString(e));
+  }
+  *plan = pl;
+  return HR_OK;
+}
+
+extern "C" int hr_bp_execute(const hr_bp_plan* pl, void* d_vol, const void* d_fp, void* stream) {
+  HR_REQUIRE(pl != nullptr && d_vol != nullptr && d_fp != nullptr, "hr_bp_execute: NULL argument");
+  const BpParams& P = pl->prm;
+  cudaStream_t s = hr::as_stream(stream);
+  if (pl->form == HR_FORM_PLAIN) {
+    dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, (P.ZN + kNzPlain - 1) / kNzPlain);
+    HR_REQUIRE(grid.z <= 65535 && grid.y <= 65535, "backprojection: grid too large");
+    bp_plain_kernel<kNzPlain><<<grid, dim3(kBx, kBy), sizeof(float) * P.N_2pi, s>>>(
+        static_cast<float*>(d_vol), static_cast<const float*>(d_fp), pl->d_views, pl->d_w, P);
+  } else {
+    dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, (P.ZN + kNzFp64 - 1) / kNzFp64);
+    HR_REQUIRE(grid.z <= 65535 && grid.y <= 65535, "backprojection: grid too large");
+    bp_fp64_kernel<kNzFp64><<<grid, dim3(kBx, kBy), sizeof(double) * P.N_2pi, s>>>(
+        static_cast<double*>(d_vol), static_cast<const double*>(d_fp), pl->d_views, pl->d_wd, P);
+  }
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
+extern "C" void hr_bp_plan_destroy(hr_bp_plan* pl) {
+  if (!pl) return;
+  cudaFree(pl->d_views);
+  cudaFree(pl->d_w);
+  cudaFree(pl->d_wd);
+  delete pl;
+}

@@ -1,0 +1,68 @@
+// Internal helpers shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+
+#include "helixrecon.h"
+
+namespace hr {
+
+// Records a printf-style message as the calling thread's last error and
+// returns `code`, so that call sites can `return fail(...)`.
+int fail(int code, const char* fmt, ...);
+void clear_error();
+
+// Checks a CUDA runtime call; on failure records file:line and the CUDA
+// message and returns HR_ERR_CUDA (HR_ERR_OUT_OF_MEMORY for allocation).
+#define HR_CUDA_TRY(expr)                                                                             \
+  do {                                                                                                \
+    cudaError_t hr_e_ = (expr);                                                                       \
+    if (hr_e_ != cudaSuccess) {                                                                       \
+      return ::hr::fail(hr_e_ == cudaErrorMemoryAllocation ? HR_ERR_OUT_OF_MEMORY : HR_ERR_CUDA,      \
+                        "%s:%d: %s failed: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(hr_e_)); \
+    }                                                                                                 \
+  } while (0)
+
+#define HR_TRY(expr)            \
+  do {                          \
+    int hr_s_ = (expr);         \
+    if (hr_s_ != HR_OK) return hr_s_; \
+  } while (0)
+
+#define HR_REQUIRE(cond, ...)                                              \
+  do {                                                                     \
+    if (!(cond)) return ::hr::fail(HR_ERR_INVALID_ARGUMENT, __VA_ARGS__); \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Checks that a CUDA device is usable; records HR_ERR_NO_DEVICE otherwise.
+int require_device();
+
+// RAII device buffer used by the host-pointer entries.
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int alloc(size_t n) {
+    bytes = n;
+    if (n == 0) return HR_OK;
+    HR_CUDA_TRY(cudaMalloc(&ptr, n));
+    return HR_OK;
+  }
+  ~DeviceBuffer() {
+    if (ptr) cudaFree(ptr);
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+}  // namespace hr

@@ -1,0 +1,155 @@
+"""Whole-scan reconstruction through the library's chain plan.
+
+``HelicalRecon`` wraps ``hr_recon_plan`` (csrc/recon.cpp), which restates the
+per-segment driver src/analyticalReconBigPatient.m:77-146 for a whole scan
+held in HBM: rebin, drop the half-fan margin at the scan ends (m-file
+:80-93), preweight + ramp filter, backproject. The plan's geometry tables and
+intermediate buffers are made once; ``run`` only enqueues kernels on a stream
+(timed or captured by the caller), ``run_host`` copies host data in and the
+volume out around it.
+
+``StagePlans`` exposes the three stage plans separately (used for the FP64
+data path and for per-stage timing).
+
+PyTorch provides device memory and streams only; all compute runs in
+libhelixrecon.so.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .geometry import Scan
+
+
+def _stream(device: torch.device, stream) -> int:
+    if stream is None:
+        return torch.cuda.current_stream(device).cuda_stream
+    return stream if isinstance(stream, int) else stream.cuda_stream
+
+
+def recon_desc(scan: Scan, w: np.ndarray, form: int) -> _lib.ReconDesc:
+    ra, fa = scan.rebin_args(), scan.filter_args()
+    return _lib.ReconDesc(YL=ra["YL"], ZL=ra["ZL"], ViewN=ra["ViewN"], YLC=ra["YLC"], dYA=ra["dYA"],
+                          DeltaTheta=ra["DeltaTheta"], PLC=ra["PLC"], DeltaT=ra["DeltaT"], DeltaFai=ra["DeltaFai"],
+                          SO=ra["SO"], view0=scan.crop_front, fPLC=fa["PLC"], fZLC=fa["ZLC"], fdYL=fa["dYL"],
+                          fdZL=fa["dZL"], fSO=fa["SO"], bp=_lib.BpGeom.from_dict(scan.bp_geom()), w=w.ctypes.data,
+                          form=form)
+
+
+def view_weights(scan: Scan) -> np.ndarray:
+    w = np.zeros(scan.N_2pi, dtype=np.float64)
+    _lib.call("hr_view_weights", w.ctypes.data, scan.N_2pi, scan.HSCoef, scan.delta)
+    return w
+
+
+class HelicalRecon:
+    """Whole-scan reconstruction on one GPU (float volume)."""
+
+    def __init__(self, scan: Scan, form: int = _lib.HR_FORM_PLAIN, device: int | torch.device = 0):
+        self.scan = scan
+        self.form = form
+        self.device = torch.device("cuda", device) if isinstance(device, int) else device
+        self._plan = ctypes.c_void_p()
+        w = view_weights(scan)
+        desc = recon_desc(scan, w, form)
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().hr_recon_plan_create(ctypes.byref(self._plan), ctypes.byref(desc)))
+        self.volume = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, device=self.device)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(_lib.load().hr_recon_device_bytes(self._plan))
+
+    def run(self, fan: torch.Tensor, volume: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """fan: device float32 [views][YL][ZL] (post-flip channel order)."""
+        vol = self.volume if volume is None else volume
+        if fan.dtype != torch.float32 or not fan.is_contiguous() or fan.numel() != self.scan.projection_bytes() // 4:
+            raise ValueError("fan must be a contiguous float32 tensor of [views][YL][ZL]")
+        _lib.check(_lib.load().hr_recon_execute(self._plan, vol.data_ptr(), fan.data_ptr(), _stream(self.device,
+                                                                                                      stream)))
+        return vol
+
+    def run_host(self, fan, volume=None):
+        """Host arrays (numpy or CPU tensors; pinned for full copy speed). Synchronous."""
+        s = self.scan
+        if volume is None:
+            volume = np.empty((s.YN, s.XN, s.ZN), dtype=np.float32)
+        fp = fan.data_ptr() if isinstance(fan, torch.Tensor) else np.ascontiguousarray(fan, np.float32).ctypes.data
+        vp = volume.data_ptr() if isinstance(volume, torch.Tensor) else volume.ctypes.data
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().hr_recon_execute_host(self._plan, vp, fp))
+        return volume
+
+    def close(self) -> None:
+        if self._plan:
+            _lib.load().hr_recon_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class StagePlans:
+    """The three stage plans of a scan, for per-stage use and the FP64 form."""
+
+    def __init__(self, scan: Scan, form: int = _lib.HR_FORM_PLAIN):
+        lib = _lib.load()
+        self.scan, self.form = scan, form
+        self._rebin, self._filter, self._bp = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        ra, fa = scan.rebin_args(), scan.filter_args()
+        _lib.check(lib.hr_rebin_plan_create(ctypes.byref(self._rebin), ra["YL"], ra["ZL"], ra["ViewN"], ra["YLC"],
+                                            ra["dYA"], ra["DeltaTheta"], ra["PLC"], ra["DeltaT"], ra["DeltaFai"],
+                                            ra["SO"]))
+        _lib.check(lib.hr_filter_plan_create(ctypes.byref(self._filter), fa["YL"], fa["ZL"], fa["ViewN"], fa["PLC"],
+                                             fa["ZLC"], fa["dYL"], fa["dZL"], fa["SO"]))
+        self.w = view_weights(scan)
+        geom = _lib.BpGeom.from_dict(scan.bp_geom())
+        _lib.check(lib.hr_bp_plan_create(ctypes.byref(self._bp), ctypes.byref(geom), self.w.ctypes.data, form))
+
+    def rebin(self, out: torch.Tensor, fan: torch.Tensor, stream: int = 0) -> None:
+        _lib.check(_lib.load().hr_rebin_execute(self._rebin, out.data_ptr(), fan.data_ptr(), stream))
+
+    def filter(self, out: torch.Tensor, inp: torch.Tensor, in_layout: int, view0: int, stream: int = 0) -> None:
+        _lib.check(_lib.load().hr_filter_execute(self._filter, out.data_ptr(), inp.data_ptr(), in_layout, view0,
+                                                 stream))
+
+    def backproject(self, vol: torch.Tensor, fp: torch.Tensor, stream: int = 0) -> None:
+        _lib.check(_lib.load().hr_bp_execute(self._bp, vol.data_ptr(), fp.data_ptr(), stream))
+
+    def close(self) -> None:
+        lib = _lib.load()
+        for attr, fn in (("_rebin", lib.hr_rebin_plan_destroy), ("_filter", lib.hr_filter_plan_destroy),
+                         ("_bp", lib.hr_bp_plan_destroy)):
+            if getattr(self, attr):
+                fn(getattr(self, attr))
+                setattr(self, attr, ctypes.c_void_p())
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def project(scan: Scan, objects: np.ndarray, out: torch.Tensor | None = None, device: int = 0) -> torch.Tensor:
+    """Analytic fan projections of a phantom on the GPU: float32 [views][YL][ZL]."""
+    from .phantom import projector_args
+
+    dev = torch.device("cuda", device)
+    a = projector_args(scan)
+    if out is None:
+        out = torch.empty((a["ViewN"], a["YL"], a["ZL"]), dtype=torch.float32, device=dev)
+    obj = torch.as_tensor(np.ascontiguousarray(objects, dtype=np.float64).reshape(-1, 17), device=dev)
+    st = torch.cuda.current_stream(dev)
+    _lib.check(_lib.load().hr_project_ellipsoids(out.data_ptr(), a["YL"], a["ZL"], a["ViewN"], a["SO"], a["SD"],
+                                                 a["dYA"], a["YLC0"], a["dZL"], a["ZLC0"], a["BetaS"], a["dBeta"],
+                                                 a["h"], obj.data_ptr(), obj.shape[0], st.cuda_stream))
+    st.synchronize()
+    return out

@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Benchmark of the helical cone-beam FBP chain on one B200 (or N, weak scaling).
+
+Workload (one step): one full-size scan -- curved detector 888 x 64, 984
+views/rotation, pitch 0.984, 20 rotations (19,680 fan views, 4.47 GB FP32) --
+rebinned, filtered and backprojected into 512 x 512 x N voxels of 0.9766 x
+0.9766 x 0.625 mm, N spanning the fully sampled z range. Synthetic data: an
+analytic FP64 projection of a seeded random-ellipsoid phantom (60 ellipsoids
+in an elliptic water cylinder), made on the GPU before timing.
+
+Metric: GUPS = voxel-view updates per second (every (voxel, view) in the
+clamped [s1, s2] window of the backprojection) for the whole chain; also
+seconds per volume. ``value`` is measured with the fan data resident in HBM;
+``e2e`` through the C ABI's host-pointer entry (hr_recon_execute_host) with
+pinned host buffers, copies inside the timed region.
+
+Multi-GPU (torchrun): every rank reconstructs its own scan (independent
+objects, weak scaling); there is no data-path collective.
+
+``--impl reference`` times the reference's own CPU implementation (its C++
+rebinning and backprojection compiled from its sources, oracle/_ref/, with the
+FP64 filter restatement since the reference has no C/C++ CPU filter) on a
+bounded sample of the same workload, on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+BYTES_PER_UPDATE_FP32 = 16  # four FP32 taps per voxel-view update
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["full", "small"], default="full")
+    ap.add_argument("--form", choices=["plain"], default="plain")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"])}, "measured"
+    return dict(PEAKS_FALLBACK), "fallback"
+
+
+def traffic_from_profiles(kernel: str, config: str):
+    """DRAM bytes per launch recorded from an ncu capture (profiles/<kernel>_<config>.md,
+    line 'dram_bytes_per_launch: N'), or None."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{config}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9 and (self.uuid is None or self.uuid in parts[0]):
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (bounded samples; the oracle and the compiled reference are the
+# checker and the baseline, never the measured product)
+# ---------------------------------------------------------------------------
+def cpu_baseline(scan, budget_s: float = 20.0, kind: str = "auto"):
+    """Reference CPU path on a bounded sample, extrapolated to one volume.
+
+    rebin: the reference's ParallelRebinningCBCurve_CPU<float> on a block of views;
+    filter: the FP64 Toeplitz restatement of the MATLAB filter on a block of rows;
+    backprojection: the reference's ParallelFDKHelical3DWeightingCPU on a sub-volume
+    of whole columns x a few slices. Each part runs on all host cores (one
+    reference call per thread on disjoint blocks). Returns (GUPS, s/volume, detail).
+    """
+    from concurrent.futures import ThreadPoolExecutor
+
+    import oracle
+
+    use_ref = oracle.ref_available() if kind == "auto" else kind == "reference"
+    ncores = os.cpu_count() or 1
+    rng = np.random.default_rng(0)
+    ra, fa, g = scan.rebin_args(), scan.filter_args(), scan.bp_geom()
+    # rebin: a block of views per thread
+    nv = max(1, min(64, ra["ViewN"] // ncores))
+    blocks = [rng.random((nv + 160, ra["YL"], ra["ZL"]), dtype=np.float32) for _ in range(ncores)]
+    a = dict(ra, ViewN=nv + 160)
+    fn = oracle.ref_rebin_f32 if use_ref else oracle.rebin_f32
+    t = time.perf_counter()
+    with ThreadPoolExecutor(ncores) as ex:
+        list(ex.map(lambda b: fn(b, **a), blocks))
+    t_rebin = (time.perf_counter() - t) * ra["ViewN"] / (ncores * (nv + 160))
+    # filter: rows of a block of views (OpenMP inside)
+    nvf = max(1, min(200, fa["ViewN"]))
+    rows = rng.standard_normal((nvf, fa["ZL"], fa["YL"]))
+    t = time.perf_counter()
+    oracle.filter_f64(rows, **dict(fa, ViewN=nvf), nthreads=ncores)
+    t_filter = (time.perf_counter() - t) * fa["ViewN"] / nvf
+    # backprojection: whole slices of a z band in the middle of the scan, split by y rows
+    w = oracle.weight_table(scan.N_2pi, scan.HSCoef, scan.delta)
+    nz = 2
+    z0 = scan.ZN // 2
+    s0 = int(np.ceil((2 * 3.14159265358979 * ((z0 - g["ZNC"]) * g["dz"]) / g["h"] - g["BetaS"]) / g["DeltaFai"] - .5))
+    lo, hi = max(0, s0 - 400), min(g["PN"], s0 + 420)
+    fp = rng.standard_normal((hi - lo, g["ZL"], g["YL"]))
+    # probe the per-update time on a small block, then size the sample to the budget
+    ny_probe = 2
+    sub = dict(g, YN=ny_probe, ZN=nz, ZNC=g["ZNC"] - z0, PN=hi - lo, BetaS=g["BetaS"] + lo * g["DeltaFai"])
+    t = time.perf_counter()
+    (oracle.ref_bp_f64 if use_ref else (lambda f, ww, gg: oracle.bp_f64(f, ww, gg, nthreads=1)))(fp, w, sub)
+    t_probe = time.perf_counter() - t
+    upd_probe = ny_probe * g["XN"] * nz * 671
+    per_upd = t_probe / upd_probe
+    ny_per_thread = max(1, min(g["YN"] // ncores, int(budget_s * 0.6 / (per_upd * g["XN"] * nz * 671))))
+    subs = []
+    for c in range(ncores):
+        y0 = c * ny_per_thread
+        subs.append(dict(sub, YN=ny_per_thread, YNC=g["YNC"] - y0))
+    bp_fn = oracle.ref_bp_f64 if use_ref else (lambda f, ww, gg: oracle.bp_f64(f, ww, gg, nthreads=1))
+    t = time.perf_counter()
+    with ThreadPoolExecutor(ncores) as ex:
+        list(ex.map(lambda gg: bp_fn(fp, w, gg), subs))
+    t_bp_sample = time.perf_counter() - t
+    upd_sample = ncores * ny_per_thread * g["XN"] * nz * 671
+    t_bp = t_bp_sample * scan.updates() / upd_sample
+    total = t_rebin + t_filter + t_bp
+    detail = {"rebin_s": t_rebin, "filter_s": t_filter, "bp_s": t_bp,
+              "sample": (f"rebin {ncores}x{nv + 160} views, filter {nvf} views x {fa['ZL']} rows, backprojection "
+                         f"{ncores}x{ny_per_thread} rows x {g['XN']} x {nz} slices (centre of the scan, "
+                         f"{upd_sample:.3g} updates); each extrapolated linearly to the full volume"),
+              "kind": "reference" if use_ref else "port", "cores": ncores}
+    return scan.updates() / total / 1e9, total, detail
+
+
+def run_reference(args, scan, rank, world):
+    if rank != 0:
+        return
+    steps = []
+    detail = None
+    for i in range(args.warmup + args.steps):
+        gups, spv, detail = cpu_baseline(scan, budget_s=8.0)
+        if i >= args.warmup:
+            steps.append((gups, spv))
+    gups = statistics.median(s[0] for s in steps)
+    spv = statistics.median(s[1] for s in steps)
+    line = {"impl": "reference", "metric": "GUPS (voxel-view updates/s, rebin+filter+3D-weighted helical BP)",
+            "value": gups, "unit": "GUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": spv * 1e3, "s_per_volume": spv, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": scan_name(scan, args.config), "flush": "n/a (CPU)"},
+            "cpu_baseline": {"value": gups, "unit": "GUPS", "cores": detail["cores"], "kind": detail["kind"],
+                             "sample": detail["sample"]},
+            "e2e": {"value": gups, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "detail": {k: detail[k] for k in ("rebin_s", "filter_s", "bp_s")}}
+    print(json.dumps(line), flush=True)
+
+
+def scan_name(scan, config):
+    return (f"helical {scan.YL}x{scan.ZL} curved detector, {scan.N_2pi} views/rot, pitch {scan.pitch}, "
+            f"{scan.rotations:g} rot ({scan.views} fan views, {scan.PN} backprojected) -> "
+            f"{scan.XN}x{scan.YN}x{scan.ZN} @ {scan.dx}x{scan.dy}x{scan.dz} mm ({config})")
+
+
+def main():
+    args = parse()
+    import torch
+    import torch.distributed as dist
+
+    from analyticalreconbigpatient_b200 import _lib, geometry as G, phantom as P
+    from analyticalreconbigpatient_b200.pipeline import HelicalRecon, StagePlans, project
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    scan = G.config(args.config)
+    if args.impl == "reference":
+        run_reference(args, scan, rank, world)
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- data (each rank its own seeded phantom) --------------------------
+    zlo = scan.h * scan.BetaS / (2 * np.pi)
+    zhi = scan.h * (scan.BetaS + scan.views * scan.dBeta) / (2 * np.pi)
+    objs = P.random_ellipsoids(1000 + rank, 60, (zlo, zhi)) if args.config == "full" else P.shepp_logan()
+    fan = project(scan, objs, device=local)
+    rec = HelicalRecon(scan, form=_lib.HR_FORM_PLAIN, device=dev)
+    stages = StagePlans(scan)
+    stream = torch.cuda.current_stream(dev)
+    st = stream.cuda_stream
+    updates = scan.updates()
+
+    # ---- per-stage timing (warm), dominant kernel = backprojection --------
+    rebinned = torch.empty((scan.views, scan.YL, scan.ZL), dtype=torch.float32, device=dev)
+    filtered = torch.empty((scan.PN, scan.ZL, scan.YL), dtype=torch.float32, device=dev)
+    vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    stage_ms = {"rebin": [], "filter": [], "backprojection": []}
+    for i in range(args.warmup + args.steps):
+        ev[0].record(stream)
+        stages.rebin(rebinned, fan, st)
+        ev[1].record(stream)
+        stages.filter(filtered, rebinned, _lib.HR_LAYOUT_REBIN, scan.crop_front, st)
+        ev[2].record(stream)
+        stages.backproject(vol, filtered, st)
+        ev[3].record(stream)
+        stream.synchronize()
+        if i >= args.warmup:
+            stage_ms["rebin"].append(ev[0].elapsed_time(ev[1]))
+            stage_ms["filter"].append(ev[1].elapsed_time(ev[2]))
+            stage_ms["backprojection"].append(ev[2].elapsed_time(ev[3]))
+    del rebinned, filtered, vol
+    stages.close()
+
+    # ---- timed whole chain (device resident) -------------------------------
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    for _ in range(args.warmup):
+        rec.run(fan, stream=st)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        rec.run(fan, stream=st)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.stop()
+    ms = t0.elapsed_time(t1) / args.steps
+    if world > 1:
+        tm = torch.tensor([ms], device=dev)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        ms = float(tm.item())
+    value = updates * world / (ms * 1e-3) / 1e9
+
+    # ---- end to end through the C ABI host entry ----------------------------
+    h_fan = torch.empty(fan.shape, dtype=torch.float32, pin_memory=True)
+    h_fan.copy_(fan)
+    h_vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, pin_memory=True)
+    del fan
+    rec.run_host(h_fan, h_vol)  # warm
+    barrier()
+    e2e_t = []
+    for _ in range(args.e2e_steps):
+        t = time.perf_counter()
+        rec.run_host(h_fan, h_vol)
+        e2e_t.append(time.perf_counter() - t)
+    e2e_s = statistics.median(e2e_t)
+    if world > 1:
+        tm = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        e2e_s = float(tm.item())
+    e2e_value = updates * world / e2e_s / 1e9
+    rec.close()
+
+    # ---- roofline of the dominant kernel -------------------------------------
+    pk, pk_kind = peaks()
+    bp_ms = statistics.mean(stage_ms["backprojection"])
+    achieved = BYTES_PER_UPDATE_FP32 * updates / (bp_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "bp_plain_kernel", "achieved": achieved, "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": pk_kind,
+                "algorithmic_bytes_per_launch": BYTES_PER_UPDATE_FP32 * updates,
+                "traffic": traffic_from_profiles("bp_plain", args.config),
+                "note": "gather-equivalent bytes (4 FP32 taps per update) / BP kernel time; BP is gather/issue "
+                        "bound, its compulsory DRAM bytes are only the filtered data and the volume"}
+
+    line = {"metric": "GUPS (voxel-view updates/s, rebin+filter+3D-weighted helical BP)", "value": value,
+            "unit": "GUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "s_per_volume": ms * 1e-3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (analytic FP64 projections of seeded random-ellipsoid phantoms)",
+            "form": args.form,
+            "config": {"workload": scan_name(scan, args.config), "updates_per_volume": updates,
+                       "parallelism": f"independent scans x{world}" if world > 1 else "1 GPU",
+                       "flush": "inputs larger than L2 (fan data 4.47 GB, filtered data 4.4 GB)"},
+            "stages_ms": {k: statistics.mean(v) for k, v in stage_ms.items()},
+            "roofline": roofline,
+            "e2e": {"value": e2e_value, "unit": "GUPS", "s_per_volume": e2e_s,
+                    "h2d_bytes_per_step": scan.projection_bytes(), "d2h_bytes_per_step": scan.volume_bytes(),
+                    "entry": "hr_recon_execute_host (C ABI, pinned host buffers)"},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks.summary()}
+    if rank == 0 and not args.no_cpu_baseline:
+        gups, spv, detail = cpu_baseline(scan)
+        line["cpu_baseline"] = {"value": gups, "unit": "GUPS", "cores": detail["cores"], "kind": detail["kind"],
+                                "sample": detail["sample"], "s_per_volume": spv}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,211 @@
+/*
+ * helixrecon.h -- C ABI of the B200-native helical cone-beam FBP chain
+ * (curved-detector fan->parallel rebinning, cosine preweight + ramp filter,
+ * 3D-weighted helical FDK backprojection).
+ *
+ * Two layers:
+ *
+ * 1. Drop-in entry points with the exact names, argument lists and array
+ *    layouts of the reference's extern "C" functions. They take HOST
+ *    pointers, are synchronous, allocate their own device memory per call and
+ *    return void, as the reference's do. They run on the calling thread's
+ *    current CUDA device (device 0 in a fresh process, which is what the
+ *    reference hard-codes). Failures are reported through hr_last_error()
+ *    and, unlike the reference, never silently: the output is left untouched
+ *    and an error message is printed to stderr.
+ *
+ * 2. hr_* entry points that return an hr_status: host-pointer twins of the
+ *    drop-ins, and plan-based device-pointer entries that take a CUDA stream
+ *    (passed as void*), allocate nothing at execute time and can be captured
+ *    into CUDA graphs.
+ *
+ * Layouts (C order, last index fastest):
+ *   fan / rebinned projections  [ViewN][YL][ZL]   (MATLAB [ZL,YL,ViewN])
+ *   filter input / output       [ViewN][ZL][YL]   (MATLAB [YL,ZL,ViewN])
+ *   volume                      [YN][XN][ZN]      (MATLAB [ZN,XN,YN])
+ */
+#ifndef HELIXRECON_H
+#define HELIXRECON_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================================================================== */
+/* 1. Reference drop-ins                                                    */
+/* ======================================================================== */
+
+/* Replaces src/ParallelRebinningCBCurve.h:4-8 / src/ParallelRebinningCBCurveGPU.cu:106-115.
+ * Fan -> parallel rebinning; YLC and PLC 0-based. Clamp rule of the reference's
+ * CPU path (src/ParallelRebinningCBCurve.cpp:55-85); result bit-identical to it. */
+void ParallelRebinningCBCurve_GPU(float* outputProj, const float* Proj, const int YL, const int ZL, const int ViewN,
+                                  const float YLC, const float dYA, const float DeltaTheta, const float PLC,
+                                  const float DeltaT, const float DeltaFai, const float SO);
+
+/* Replaces src/filtering.h:12-18 / src/filtering.cu:270-287. Cosine preweight and
+ * Shepp-Logan ramp filter of every detector row, cuFFT-free (own radix-4 FFT). */
+void filtering(float* hfpwd, const float* hProj, const int YL, const int ZL, const int ViewN, const float PLC,
+               const float ZLC, const float dYL, const float dZL, const float SO);
+
+/* Replaces src/ParallelFDKHelical3DWeightingGPU.h:4-13 / ...GPU.cu:421-436.
+ * FP64 data path on the GPU; views s1..s2 as the reference's CPU loop. */
+void ParallekFDKHelical3DWeighting_GPU_double(
+    double* hctimage, const double* hfp, const double* hw, const int N_2pi, const int XN, const int YN,
+    const int ZN, const double XNC, const double YNC, const double ZNC, const double dx, const double dy,
+    const double dz, const int YL, const int ZL, const int PN, const double YLC, const double ZLC,
+    const double dYL, const double dZL, const double h, const double BetaS, const double DeltaFai,
+    const double N_pi, const double HSCoef, const double SO, const double SD, const double k1);
+
+/* Replaces src/ParallelFDKHelical3DWeightingGPU.h:15-24 / ...GPU.cu:440-455.
+ * FP32 data path; view/row/channel index selection computed in FP64 with the
+ * reference CPU's expression order, so it is bit-exact to that path. */
+void ParallekFDKHelical3DWeighting_GPU_float(
+    float* hctimage, const float* hfp, const float* hw, const int N_2pi, const int XN, const int YN, const int ZN,
+    const float XNC, const float YNC, const float ZNC, const float dx, const float dy, const float dz,
+    const int YL, const int ZL, const int PN, const float YLC, const float ZLC, const float dYL, const float dZL,
+    const float h, const float BetaS, const float DeltaFai, const float N_pi, const float HSCoef, const float SO,
+    const float SD, const float k1);
+
+/* Replaces src/Parallel_FDK_Helical_3DWeighting.cpp:117-200. Derives dx,dy,dz,
+ * dYL,dZL,DeltaFai and the view weight w as the reference does. useGPU == 1
+ * runs the FP32 data path (as the reference's GPU branch); any other value
+ * runs the FP64 data path on the GPU (the reference's CPU branch semantics). */
+void ParallelFDKHelical3DWeighting(double* ctimage, const double* fp, const double SO, const double DO,
+                                   const int YL, const int ZL, const double DecWidth, const double DecHeigh,
+                                   const double YLC, const double ZLC, const double h, const double BetaS,
+                                   const int PN, const int N_2pi, const double ObjR, const int XN, const int YN,
+                                   const int ZN, const double XNC, const double YNC, const double ZNC,
+                                   const int delta, const double HSCoef, const double k1, const int useGPU);
+
+/* ======================================================================== */
+/* 2. Status-returning API                                                  */
+/* ======================================================================== */
+
+typedef enum hr_status {
+  HR_OK = 0,
+  HR_ERR_INVALID_ARGUMENT = 1,
+  HR_ERR_CUDA = 2,
+  HR_ERR_OUT_OF_MEMORY = 3,
+  HR_ERR_NO_DEVICE = 4,
+  HR_ERR_UNSUPPORTED = 5
+} hr_status;
+
+/* Precision forms of the chain. */
+typedef enum hr_form {
+  HR_FORM_PLAIN = 0, /* FP32 data, FFT filter, FP64 exact index selection (the drop-in) */
+  HR_FORM_FP64 = 1,  /* FP64 data path */
+  HR_FORM_FAST = 2   /* BF16 split Toeplitz filter on tcgen05, BF16 filtered data, fast BP */
+} hr_form;
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char* hr_last_error(void);
+/* Library version (major*10000 + minor*100 + patch). */
+int hr_version(void);
+
+/* Host-pointer twins of the drop-ins. Same arguments; return an hr_status. */
+int hr_rebin_host(float* outputProj, const float* Proj, int YL, int ZL, int ViewN, float YLC, float dYA,
+                  float DeltaTheta, float PLC, float DeltaT, float DeltaFai, float SO);
+int hr_filter_host(float* hfpwd, const float* hProj, int YL, int ZL, int ViewN, float PLC, float ZLC, float dYL,
+                   float dZL, float SO);
+int hr_bp_host_float(float* hctimage, const float* hfp, const float* hw, int N_2pi, int XN, int YN, int ZN,
+                     float XNC, float YNC, float ZNC, float dx, float dy, float dz, int YL, int ZL, int PN,
+                     float YLC, float ZLC, float dYL, float dZL, float h, float BetaS, float DeltaFai, float N_pi,
+                     float HSCoef, float SO, float SD, float k1);
+int hr_bp_host_double(double* hctimage, const double* hfp, const double* hw, int N_2pi, int XN, int YN, int ZN,
+                      double XNC, double YNC, double ZNC, double dx, double dy, double dz, int YL, int ZL, int PN,
+                      double YLC, double ZLC, double dYL, double dZL, double h, double BetaS, double DeltaFai,
+                      double N_pi, double HSCoef, double SO, double SD, double k1);
+/* Status twin of ParallelFDKHelical3DWeighting (same arguments). */
+int hr_bp_host_reference(double* ctimage, const double* fp, double SO, double DO, int YL, int ZL, double DecWidth,
+                         double DecHeigh, double YLC, double ZLC, double h, double BetaS, int PN, int N_2pi,
+                         double ObjR, int XN, int YN, int ZN, double XNC, double YNC, double ZNC, int delta,
+                         double HSCoef, double k1, int useGPU);
+
+/* View weight table w[N_2pi] of src/Parallel_FDK_Helical_3DWeighting.cpp:156-170
+ * (cos^2 tapers of `delta` views at both ends of a 2 ceil(N_pi HSCoef)+1 window). */
+int hr_view_weights(double* w, int N_2pi, double HSCoef, int delta);
+
+/* ---- rebinning plan ----------------------------------------------------- */
+typedef struct hr_rebin_plan hr_rebin_plan;
+int hr_rebin_plan_create(hr_rebin_plan** plan, int YL, int ZL, int ViewN, float YLC, float dYA, float DeltaTheta,
+                         float PLC, float DeltaT, float DeltaFai, float SO);
+/* d_out, d_proj: device [ViewN][YL][ZL]. */
+int hr_rebin_execute(const hr_rebin_plan* plan, float* d_out, const float* d_proj, void* stream);
+void hr_rebin_plan_destroy(hr_rebin_plan* plan);
+
+/* ---- filter plan -------------------------------------------------------- */
+typedef struct hr_filter_plan hr_filter_plan;
+/* Input layouts for hr_filter_execute. */
+#define HR_LAYOUT_ROWS 0   /* [views][ZL][YL] (YL fastest), the reference filter layout */
+#define HR_LAYOUT_REBIN 1  /* [views][YL][ZL] (ZL fastest), the rebinning output */
+int hr_filter_plan_create(hr_filter_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC, float dYL,
+                          float dZL, float SO);
+/* Filters views [view0, view0+ViewN) of d_in (laid out as in_layout, holding
+ * at least view0+ViewN views) into d_out [ViewN][ZL][YL]. */
+int hr_filter_execute(const hr_filter_plan* plan, float* d_out, const float* d_in, int in_layout, int view0,
+                      void* stream);
+void hr_filter_plan_destroy(hr_filter_plan* plan);
+
+/* ---- backprojection plan ------------------------------------------------ */
+typedef struct hr_bp_geom {
+  int N_2pi, XN, YN, ZN, YL, ZL, PN;
+  double XNC, YNC, ZNC, dx, dy, dz;
+  double YLC, ZLC, dYL, dZL, h, BetaS, DeltaFai, N_pi, HSCoef, SO, SD, k1;
+} hr_bp_geom;
+
+typedef struct hr_bp_plan hr_bp_plan;
+/* w: host view weight table of N_2pi entries (as the reference's hw). form:
+ * HR_FORM_PLAIN (fp float), HR_FORM_FP64 (fp double). */
+int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const double* w, int form);
+/* d_fp: device [PN][ZL][YL] (float, or double for HR_FORM_FP64);
+ * d_vol: device [YN][XN][ZN] of the same type. */
+int hr_bp_execute(const hr_bp_plan* plan, void* d_vol, const void* d_fp, void* stream);
+void hr_bp_plan_destroy(hr_bp_plan* plan);
+
+/* ---- whole chain: rebin -> crop -> preweight/filter -> backprojection ---- */
+/* The per-scan driver of src/analyticalReconBigPatient.m:77-146 as one plan. */
+typedef struct hr_recon_desc {
+  /* rebinning: the arguments of ParallelRebinningCBCurve_GPU (YLC, PLC 0-based) */
+  int YL, ZL, ViewN;
+  float YLC, dYA, DeltaTheta, PLC, DeltaT, DeltaFai, SO;
+  /* rebinned views [view0, view0 + bp.PN) are filtered and backprojected (the
+   * segment-overlap crop of the m-file :80-93) */
+  int view0;
+  /* filter: the arguments of `filtering` (PLC, ZLC 0-based) */
+  float fPLC, fZLC, fdYL, fdZL, fSO;
+  /* backprojection geometry; bp.YL/ZL must equal YL/ZL */
+  hr_bp_geom bp;
+  const double* w; /* N_2pi view weights, copied at plan creation */
+  int form;        /* hr_form */
+} hr_recon_desc;
+
+typedef struct hr_recon_plan hr_recon_plan;
+int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* desc);
+/* Device pointers: d_fan [ViewN][YL][ZL] float, d_vol [YN][XN][ZN] float. */
+int hr_recon_execute(const hr_recon_plan* plan, float* d_vol, const float* d_fan, void* stream);
+/* Host pointers (pinned for full copy speed): copies the fan data in, runs the
+ * chain, copies the volume out; returns when h_vol is written. */
+int hr_recon_execute_host(hr_recon_plan* plan, float* h_vol, const float* h_fan);
+/* Device bytes the plan holds (tables + intermediate + host-staging buffers). */
+size_t hr_recon_device_bytes(const hr_recon_plan* plan);
+void hr_recon_plan_destroy(hr_recon_plan* plan);
+
+/* ---- analytic phantom projector (synthetic data source) ----------------- */
+/* Objects: nobj rows of 17 doubles [type, cx, cy, cz, a, b, c, R(9, row-major,
+ * columns = body axes), mu]; type 0 ellipsoid, type 1 elliptic cylinder (z in
+ * cz +- c). Writes FP64 line integrals rounded to float into device
+ * d_proj [ViewN][YL][ZL] for the fan geometry (source angle BetaS + i*dBeta,
+ * fan angle (j - YLC0)*dYA, row rise (k - ZLC0)*dZL over SD, source height
+ * h*angle/(2 pi)). d_obj: device copy of the object table. */
+int hr_project_ellipsoids(float* d_proj, int YL, int ZL, int ViewN, double SO, double SD, double dYA, double YLC0,
+                          double dZL, double ZLC0, double BetaS, double dBeta, double h, const double* d_obj,
+                          int nobj, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HELIXRECON_H */
