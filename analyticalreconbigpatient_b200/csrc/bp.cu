@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "hr_internal.h"
+#include "bp_fast.h"
 
 namespace {
 
@@ -55,6 +56,8 @@ struct hr_bp_plan {
   ViewTab* d_views;
   float* d_w;
   double* d_wd;
+  hr::BpFastGeom fg;
+  hr::BpFast fast;
 };
 
 namespace {
@@ -259,7 +262,8 @@ extern "C" int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const d
   hr::clear_error();
   HR_REQUIRE(plan != nullptr && g != nullptr && w != nullptr, "hr_bp_plan_create: NULL argument");
   *plan = nullptr;
-  HR_REQUIRE(form == HR_FORM_PLAIN || form == HR_FORM_FP64, "hr_bp_plan_create: form %d not handled here", form);
+  HR_REQUIRE(form == HR_FORM_PLAIN || form == HR_FORM_FP64 || form == HR_FORM_FAST,
+             "hr_bp_plan_create: unknown form %d", form);
   HR_REQUIRE(g->XN > 0 && g->YN > 0 && g->ZN > 0 && g->YL > 1 && g->ZL > 1 && g->PN > 0 && g->N_2pi > 1,
              "backprojection: invalid sizes");
   HR_REQUIRE(g->h != 0.0 && g->DeltaFai != 0.0 && g->dYL != 0.0 && g->dZL != 0.0 && g->SO > 0.0,
@@ -296,7 +300,22 @@ extern "C" int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const d
   std::vector<float> wf(g->N_2pi);
   for (int i = 0; i < g->N_2pi; ++i) wf[i] = (float)w[i];
 
-  hr_bp_plan* pl = new hr_bp_plan{P, form, nullptr, nullptr, nullptr};
+  hr_bp_plan* pl = new hr_bp_plan{P, form, nullptr, nullptr, nullptr, hr::BpFastGeom{}, hr::BpFast{}};
+  if (form == HR_FORM_FAST) {
+    hr::BpFastGeom& f = pl->fg;
+    f.XN = g->XN; f.YN = g->YN; f.ZN = g->ZN; f.YL = g->YL; f.ZL = g->ZL; f.PN = g->PN; f.half = half;
+    f.XNC = g->XNC; f.YNC = g->YNC; f.ZNC = g->ZNC; f.dx = g->dx; f.dy = g->dy; f.dz = g->dz;
+    f.YLC = g->YLC; f.ZLC = g->ZLC; f.dYL = g->dYL; f.dZL = g->dZL; f.h = g->h; f.BetaS = g->BetaS;
+    f.DeltaFai = g->DeltaFai; f.N_pi = g->N_pi; f.SO = g->SO; f.SD = g->SD; f.k1 = g->k1;
+    const int st = hr::bp_fast_create(&pl->fast, f, w);
+    if (st != HR_OK) {
+      hr::bp_fast_destroy(&pl->fast);
+      delete pl;
+      return st;
+    }
+    *plan = pl;
+    return HR_OK;
+  }
   cudaError_t e = cudaMalloc(&pl->d_views, sizeof(ViewTab) * g->PN);
   if (e == cudaSuccess) e = cudaMalloc(&pl->d_w, sizeof(float) * g->N_2pi);
   if (e == cudaSuccess) e = cudaMalloc(&pl->d_wd, sizeof(double) * g->N_2pi);
@@ -319,6 +338,8 @@ extern "C" int hr_bp_execute(const hr_bp_plan* pl, void* d_vol, const void* d_fp
   HR_REQUIRE(pl != nullptr && d_vol != nullptr && d_fp != nullptr, "hr_bp_execute: NULL argument");
   const BpParams& P = pl->prm;
   cudaStream_t s = hr::as_stream(stream);
+  if (pl->form == HR_FORM_FAST)
+    return hr::bp_fast_execute(pl->fast, pl->fg, static_cast<float*>(d_vol), static_cast<const uint32_t*>(d_fp), s);
   if (pl->form == HR_FORM_PLAIN) {
     dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, (P.ZN + kNzPlain - 1) / kNzPlain);
     HR_REQUIRE(grid.z <= 65535 && grid.y <= 65535, "backprojection: grid too large");
@@ -336,6 +357,7 @@ extern "C" int hr_bp_execute(const hr_bp_plan* pl, void* d_vol, const void* d_fp
 
 extern "C" void hr_bp_plan_destroy(hr_bp_plan* pl) {
   if (!pl) return;
+  hr::bp_fast_destroy(&pl->fast);
   cudaFree(pl->d_views);
   cudaFree(pl->d_w);
   cudaFree(pl->d_wd);

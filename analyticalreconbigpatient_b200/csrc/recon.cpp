@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "hr_internal.h"
+#include "bp_fast.h"
 
 struct hr_recon_plan {
   hr_recon_desc d;
@@ -18,6 +19,7 @@ struct hr_recon_plan {
   hr_bp_plan* bp = nullptr;
   float* d_rebinned = nullptr;  // [ViewN][YL][ZL]
   float* d_filtered = nullptr;  // [PN][ZL][YL]
+  uint32_t* d_pairs = nullptr;  // [PN][ZL][YL] BF16 channel pairs (fast form)
   float* d_fan = nullptr;       // staging for host execution
   float* d_vol = nullptr;
   cudaStream_t stream = nullptr;
@@ -33,6 +35,7 @@ void destroy(hr_recon_plan* p) {
   hr_bp_plan_destroy(p->bp);
   cudaFree(p->d_rebinned);
   cudaFree(p->d_filtered);
+  cudaFree(p->d_pairs);
   cudaFree(p->d_fan);
   cudaFree(p->d_vol);
   if (p->stream) cudaStreamDestroy(p->stream);
@@ -51,8 +54,9 @@ extern "C" int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* d
   hr::clear_error();
   HR_REQUIRE(plan != nullptr && d != nullptr && d->w != nullptr, "hr_recon_plan_create: NULL argument");
   *plan = nullptr;
-  HR_REQUIRE(d->form == HR_FORM_PLAIN, "hr_recon_plan_create: form %d not available for the whole chain (the FP64 "
-             "data path is reached through the stage plans)", d->form);
+  HR_REQUIRE(d->form == HR_FORM_PLAIN || d->form == HR_FORM_FAST,
+             "hr_recon_plan_create: form %d not available for the whole chain (the FP64 data path is reached "
+             "through the stage plans)", d->form);
   HR_REQUIRE(d->bp.YL == d->YL && d->bp.ZL == d->ZL, "hr_recon_plan_create: bp.YL/ZL differ from YL/ZL");
   HR_REQUIRE(d->view0 >= 0 && d->view0 + d->bp.PN <= d->ViewN,
              "hr_recon_plan_create: views [%d, %d) exceed the %d rebinned views", d->view0, d->view0 + d->bp.PN,
@@ -70,6 +74,7 @@ extern "C" int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* d
   const size_t nvol = (size_t)d->bp.XN * d->bp.YN * d->bp.ZN;
   if (st == HR_OK) st = alloc(p, (void**)&p->d_rebinned, nfan * sizeof(float));
   if (st == HR_OK) st = alloc(p, (void**)&p->d_filtered, nfilt * sizeof(float));
+  if (st == HR_OK && d->form == HR_FORM_FAST) st = alloc(p, (void**)&p->d_pairs, nfilt * sizeof(uint32_t));
   if (st == HR_OK) st = alloc(p, (void**)&p->d_fan, nfan * sizeof(float));
   if (st == HR_OK) st = alloc(p, (void**)&p->d_vol, nvol * sizeof(float));
   if (st == HR_OK) {
@@ -88,6 +93,11 @@ extern "C" int hr_recon_execute(const hr_recon_plan* p, float* d_vol, const floa
   HR_REQUIRE(p != nullptr && d_vol != nullptr && d_fan != nullptr, "hr_recon_execute: NULL argument");
   HR_TRY(hr_rebin_execute(p->rebin, p->d_rebinned, d_fan, stream));
   HR_TRY(hr_filter_execute(p->filter, p->d_filtered, p->d_rebinned, HR_LAYOUT_REBIN, p->d.view0, stream));
+  if (p->d.form == HR_FORM_FAST) {
+    HR_TRY(hr::pack_pairs(p->d_pairs, p->d_filtered, (long long)p->d.ZL * p->d.bp.PN, p->d.YL,
+                          hr::as_stream(stream)));
+    return hr_bp_execute(p->bp, d_vol, p->d_pairs, stream);
+  }
   return hr_bp_execute(p->bp, d_vol, p->d_filtered, stream);
 }
 

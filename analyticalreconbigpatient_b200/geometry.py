@@ -257,7 +257,8 @@ def config(name: str) -> Scan:
 def tiny(**kw) -> Scan:
     """A scaled-down scan for CPU-speed tests: same detector geometry family with
     fewer channels, rows and views."""
-    base = dict(SO=541.0, SD=949.0, YL=96, det_pitch=1.0239 * 888 / 96, ZL=8, row_height=1.0963, N_2pi=120,
-                pitch=0.9375, rotations=3, XN=24, YN=24, ZN=6, dx=12.0, dy=12.0, dz=1.5)
+    base = dict(SO=541.0, SD=949.0, YL=96, ZL=8, row_height=1.0963, N_2pi=120, pitch=0.9375, rotations=3, XN=24,
+                YN=24, ZN=6, dx=12.0, dy=12.0, dz=1.5)
     base.update(kw)
+    base.setdefault("det_pitch", 1.0239 * 888 / base["YL"])  # keep the full detector's fan angle
     return Scan(**base)

@@ -123,6 +123,11 @@ class StagePlans:
     def backproject(self, vol: torch.Tensor, fp: torch.Tensor, stream: int = 0) -> None:
         _lib.check(_lib.load().hr_bp_execute(self._bp, vol.data_ptr(), fp.data_ptr(), stream))
 
+    def pack(self, out: torch.Tensor, filtered: torch.Tensor, stream: int = 0) -> None:
+        """FP32 filtered rows -> BF16 channel pairs (the fast form's layout)."""
+        s = self.scan
+        _lib.check(_lib.load().hr_pack_bf16_pairs(out.data_ptr(), filtered.data_ptr(), s.ZL * s.PN, s.YL, stream))
+
     def close(self) -> None:
         lib = _lib.load()
         for attr, fn in (("_rebin", lib.hr_rebin_plan_destroy), ("_filter", lib.hr_filter_plan_destroy),

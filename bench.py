@@ -40,6 +40,7 @@ sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 BYTES_PER_UPDATE_FP32 = 16  # four FP32 taps per voxel-view update
+BYTES_PER_UPDATE_BF16 = 8   # four BF16 taps per voxel-view update
 
 
 def parse():
@@ -49,7 +50,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=["full", "small"], default="full")
-    ap.add_argument("--form", choices=["plain"], default="plain")
+    ap.add_argument("--form", choices=["fast", "plain"], default="fast",
+                    help="form timed as `value` (the chosen BF16 form by default); the plain FP32 form is "
+                         "timed beside it unless --no-plain")
+    ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     return ap.parse_args()
@@ -230,13 +234,99 @@ def scan_name(scan, config):
             f"{scan.XN}x{scan.YN}x{scan.ZN} @ {scan.dx}x{scan.dy}x{scan.dz} mm ({config})")
 
 
+def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
+    """Stage split, device-resident whole-chain timing and (optionally) e2e for one form."""
+    import torch
+    import torch.distributed as dist
+
+    from analyticalreconbigpatient_b200 import _lib
+    from analyticalreconbigpatient_b200.pipeline import HelicalRecon, StagePlans
+
+    stream = torch.cuda.current_stream(dev)
+    st = stream.cuda_stream
+    fast = form == _lib.HR_FORM_FAST
+    # ---- per-stage timing (warm) ---------------------------------------------
+    stages = StagePlans(scan, form)
+    rebinned = torch.empty((scan.views, scan.YL, scan.ZL), dtype=torch.float32, device=dev)
+    filtered = torch.empty((scan.PN, scan.ZL, scan.YL), dtype=torch.float32, device=dev)
+    pairs = torch.empty((scan.PN, scan.ZL, scan.YL), dtype=torch.int32, device=dev) if fast else None
+    vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    names = ["rebin", "filter", "pack", "backprojection"]
+    stage_ms = {k: [] for k in names}
+    for i in range(args.warmup + args.steps):
+        ev[0].record(stream)
+        stages.rebin(rebinned, fan, st)
+        ev[1].record(stream)
+        stages.filter(filtered, rebinned, _lib.HR_LAYOUT_REBIN, scan.crop_front, st)
+        ev[2].record(stream)
+        if fast:
+            stages.pack(pairs, filtered, st)
+        ev[3].record(stream)
+        stages.backproject(vol, pairs if fast else filtered, st)
+        ev[4].record(stream)
+        stream.synchronize()
+        if i >= args.warmup:
+            for k in range(4):
+                stage_ms[names[k]].append(ev[k].elapsed_time(ev[k + 1]))
+    del rebinned, filtered, pairs, vol
+    stages.close()
+    torch.cuda.empty_cache()
+
+    # ---- timed whole chain (device resident) ---------------------------------
+    rec = HelicalRecon(scan, form=form, device=dev)
+    for _ in range(args.warmup):
+        rec.run(fan, stream=st)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        rec.run(fan, stream=st)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / args.steps
+    if world > 1:
+        tm = torch.tensor([ms], device=dev)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        ms = float(tm.item())
+    out = {"ms_per_step": ms, "stages_ms": {k: statistics.mean(v) for k, v in stage_ms.items() if v},
+           "launches_per_step": 4 if fast else 3}
+
+    # ---- end to end through the C ABI host entry -----------------------------
+    if with_e2e:
+        h_fan = torch.empty(fan.shape, dtype=torch.float32, pin_memory=True)
+        h_fan.copy_(fan)
+        h_vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, pin_memory=True)
+        rec.run_host(h_fan, h_vol)  # warm
+        barrier()
+        e2e_t = []
+        for _ in range(args.e2e_steps):
+            t = time.perf_counter()
+            rec.run_host(h_fan, h_vol)
+            e2e_t.append(time.perf_counter() - t)
+        e2e_s = statistics.median(e2e_t)
+        if world > 1:
+            tm = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+            e2e_s = float(tm.item())
+        out["e2e_s"] = e2e_s
+        del h_fan, h_vol
+    rec.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     args = parse()
     import torch
     import torch.distributed as dist
 
     from analyticalreconbigpatient_b200 import _lib, geometry as G, phantom as P
-    from analyticalreconbigpatient_b200.pipeline import HelicalRecon, StagePlans, project
+    from analyticalreconbigpatient_b200.pipeline import project
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -256,114 +346,66 @@ def main():
         if world > 1:
             dist.barrier()
 
-    # ---- data (each rank its own seeded phantom) --------------------------
+    # ---- data (each rank its own seeded phantom) ------------------------------
     zlo = scan.h * scan.BetaS / (2 * np.pi)
     zhi = scan.h * (scan.BetaS + scan.views * scan.dBeta) / (2 * np.pi)
     objs = P.random_ellipsoids(1000 + rank, 60, (zlo, zhi)) if args.config == "full" else P.shepp_logan()
     fan = project(scan, objs, device=local)
-    rec = HelicalRecon(scan, form=_lib.HR_FORM_PLAIN, device=dev)
-    stages = StagePlans(scan)
-    stream = torch.cuda.current_stream(dev)
-    st = stream.cuda_stream
     updates = scan.updates()
+    chosen = _lib.HR_FORM_FAST if args.form == "fast" else _lib.HR_FORM_PLAIN
 
-    # ---- per-stage timing (warm), dominant kernel = backprojection --------
-    rebinned = torch.empty((scan.views, scan.YL, scan.ZL), dtype=torch.float32, device=dev)
-    filtered = torch.empty((scan.PN, scan.ZL, scan.YL), dtype=torch.float32, device=dev)
-    vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, device=dev)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    stage_ms = {"rebin": [], "filter": [], "backprojection": []}
-    for i in range(args.warmup + args.steps):
-        ev[0].record(stream)
-        stages.rebin(rebinned, fan, st)
-        ev[1].record(stream)
-        stages.filter(filtered, rebinned, _lib.HR_LAYOUT_REBIN, scan.crop_front, st)
-        ev[2].record(stream)
-        stages.backproject(vol, filtered, st)
-        ev[3].record(stream)
-        stream.synchronize()
-        if i >= args.warmup:
-            stage_ms["rebin"].append(ev[0].elapsed_time(ev[1]))
-            stage_ms["filter"].append(ev[1].elapsed_time(ev[2]))
-            stage_ms["backprojection"].append(ev[2].elapsed_time(ev[3]))
-    del rebinned, filtered, vol
-    stages.close()
-
-    # ---- timed whole chain (device resident) -------------------------------
     uuid = None
     try:
         uuid = str(torch.cuda.get_device_properties(dev).uuid)
     except Exception:
         pass
     clocks = ClockSampler(uuid)
-    for _ in range(args.warmup):
-        rec.run(fan, stream=st)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
     clocks.start()
-    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    for _ in range(args.steps):
-        rec.run(fan, stream=st)
-    t1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
+    res = measure_form(args, scan, chosen, fan, dev, world, barrier)
     clocks.stop()
-    ms = t0.elapsed_time(t1) / args.steps
-    if world > 1:
-        tm = torch.tensor([ms], device=dev)
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        ms = float(tm.item())
-    value = updates * world / (ms * 1e-3) / 1e9
-
-    # ---- end to end through the C ABI host entry ----------------------------
-    h_fan = torch.empty(fan.shape, dtype=torch.float32, pin_memory=True)
-    h_fan.copy_(fan)
-    h_vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, pin_memory=True)
+    plain = None
+    if chosen != _lib.HR_FORM_PLAIN and not args.no_plain:
+        plain = measure_form(args, scan, _lib.HR_FORM_PLAIN, fan, dev, world, barrier, with_e2e=False)
     del fan
-    rec.run_host(h_fan, h_vol)  # warm
-    barrier()
-    e2e_t = []
-    for _ in range(args.e2e_steps):
-        t = time.perf_counter()
-        rec.run_host(h_fan, h_vol)
-        e2e_t.append(time.perf_counter() - t)
-    e2e_s = statistics.median(e2e_t)
-    if world > 1:
-        tm = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        e2e_s = float(tm.item())
-    e2e_value = updates * world / e2e_s / 1e9
-    rec.close()
+    ms = res["ms_per_step"]
+    value = updates * world / (ms * 1e-3) / 1e9
+    e2e_value = updates * world / res["e2e_s"] / 1e9
 
-    # ---- roofline of the dominant kernel -------------------------------------
+    # ---- roofline of the dominant kernel ----------------------------------------
     pk, pk_kind = peaks()
-    bp_ms = statistics.mean(stage_ms["backprojection"])
-    achieved = BYTES_PER_UPDATE_FP32 * updates / (bp_ms * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "bp_plain_kernel", "achieved": achieved, "peak": pk["hbm_gbs"],
+    bp_ms = res["stages_ms"]["backprojection"]
+    bytes_per_update = BYTES_PER_UPDATE_BF16 if chosen == _lib.HR_FORM_FAST else BYTES_PER_UPDATE_FP32
+    kname = "bp_fast_kernel" if chosen == _lib.HR_FORM_FAST else "bp_plain_kernel"
+    achieved = bytes_per_update * updates / (bp_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": pk_kind,
-                "algorithmic_bytes_per_launch": BYTES_PER_UPDATE_FP32 * updates,
-                "traffic": traffic_from_profiles("bp_plain", args.config),
-                "note": "gather-equivalent bytes (4 FP32 taps per update) / BP kernel time; BP is gather/issue "
-                        "bound, its compulsory DRAM bytes are only the filtered data and the volume"}
+                "algorithmic_bytes_per_launch": bytes_per_update * updates,
+                "bytes_per_update": bytes_per_update,
+                "traffic": traffic_from_profiles(kname.replace("_kernel", ""), args.config),
+                "note": "gather-equivalent bytes (4 taps per update: 16 B FP32, 8 B BF16) / backprojection kernel "
+                        "time; the backprojection is gather/issue bound, its compulsory DRAM bytes are only the "
+                        "filtered data and the volume"}
 
     line = {"metric": "GUPS (voxel-view updates/s, rebin+filter+3D-weighted helical BP)", "value": value,
             "unit": "GUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "s_per_volume": ms * 1e-3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (analytic FP64 projections of seeded random-ellipsoid phantoms)",
+            "dtype": "bf16" if chosen == _lib.HR_FORM_FAST else "f32",
+            "data": "synthetic (analytic FP64 projections of seeded random-ellipsoid phantoms)",
             "form": args.form,
             "config": {"workload": scan_name(scan, args.config), "updates_per_volume": updates,
                        "parallelism": f"independent scans x{world}" if world > 1 else "1 GPU",
                        "flush": "inputs larger than L2 (fan data 4.47 GB, filtered data 4.4 GB)"},
-            "stages_ms": {k: statistics.mean(v) for k, v in stage_ms.items()},
+            "stages_ms": res["stages_ms"],
             "roofline": roofline,
-            "e2e": {"value": e2e_value, "unit": "GUPS", "s_per_volume": e2e_s,
+            "e2e": {"value": e2e_value, "unit": "GUPS", "s_per_volume": res["e2e_s"],
                     "h2d_bytes_per_step": scan.projection_bytes(), "d2h_bytes_per_step": scan.volume_bytes(),
                     "entry": "hr_recon_execute_host (C ABI, pinned host buffers)"},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": res["launches_per_step"] * args.steps,
             "clocks": clocks.summary()}
+    if plain is not None:
+        pv = updates * world / (plain["ms_per_step"] * 1e-3) / 1e9
+        line["plain"] = {"value": pv, "unit": "GUPS", "ms_per_step": plain["ms_per_step"],
+                         "stages_ms": plain["stages_ms"], "speedup_of_chosen": value / pv}
     if rank == 0 and not args.no_cpu_baseline:
         gups, spv, detail = cpu_baseline(scan)
         line["cpu_baseline"] = {"value": gups, "unit": "GUPS", "cores": detail["cores"], "kind": detail["kind"],

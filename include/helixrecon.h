@@ -158,12 +158,19 @@ typedef struct hr_bp_geom {
 
 typedef struct hr_bp_plan hr_bp_plan;
 /* w: host view weight table of N_2pi entries (as the reference's hw). form:
- * HR_FORM_PLAIN (fp float), HR_FORM_FP64 (fp double). */
+ * HR_FORM_PLAIN (fp float), HR_FORM_FP64 (fp double), HR_FORM_FAST (fp BF16
+ * channel pairs, see hr_pack_bf16_pairs). */
 int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const double* w, int form);
-/* d_fp: device [PN][ZL][YL] (float, or double for HR_FORM_FP64);
- * d_vol: device [YN][XN][ZN] of the same type. */
+/* d_fp: device [PN][ZL][YL] (float; double for HR_FORM_FP64; uint32 BF16 pairs
+ * for HR_FORM_FAST); d_vol: device [YN][XN][ZN] (double for HR_FORM_FP64, else float). */
 int hr_bp_execute(const hr_bp_plan* plan, void* d_vol, const void* d_fp, void* stream);
 void hr_bp_plan_destroy(hr_bp_plan* plan);
+
+/* ---- BF16 channel pairs (the fast form's filtered-data layout) ---------- */
+/* d_out[r][u] = bf16(d_in[r][u]) | bf16(d_in[r][u+1]) << 16 (round to nearest
+ * even; channel YL pairs with 0), for rows r in [0, rows). The fast form's
+ * backprojection plan reads this layout. */
+int hr_pack_bf16_pairs(uint32_t* d_out, const float* d_in, long long rows, int YL, void* stream);
 
 /* ---- whole chain: rebin -> crop -> preweight/filter -> backprojection ---- */
 /* The per-scan driver of src/analyticalReconBigPatient.m:77-146 as one plan. */

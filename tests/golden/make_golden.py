@@ -6,7 +6,7 @@
   Run where the reference sources exist:  python tests/golden/make_golden.py
 * filter_*.npz: the reference's own cuFFT filter (src/filtering.cu, built
   unmodified into oracle/_ref/libref_gpu.so); needs a CUDA device:
-  python tests/golden/make_golden.py --filter
+  python tests/golden/make_golden.py --filter [--out DIR]
 
 Inputs are seeded and stored with the outputs so that a check does not depend
 on regenerating them bit-for-bit elsewhere.
@@ -63,7 +63,7 @@ def make_cpu() -> None:
         print("wrote", name, "rebin", proj.shape, "bp", vol.shape)
 
 
-def make_filter() -> None:
+def make_filter(out_dir: str = HERE) -> None:
     import ctypes  # noqa: F401
 
     L = oracle.ref_gpu()
@@ -75,7 +75,7 @@ def make_filter() -> None:
         out = np.zeros_like(proj)
         L.ref_gpu_filtering(out.ctypes.data, proj.ctypes.data, fa["YL"], fa["ZL"], fa["ViewN"], fa["PLC"], fa["ZLC"],
                             fa["dYL"], fa["dZL"], fa["SO"])
-        np.savez_compressed(os.path.join(HERE, f"filter_{name}.npz"), proj=proj, out=out,
+        np.savez_compressed(os.path.join(out_dir, f"filter_{name}.npz"), proj=proj, out=out,
                             args=np.array([fa[k] for k in ("PLC", "ZLC", "dYL", "dZL", "SO")], dtype=np.float32),
                             sizes=np.array([fa["YL"], fa["ZL"], fa["ViewN"]], dtype=np.int64))
         print("wrote filter", name, proj.shape, float(np.abs(out).max()))
@@ -83,6 +83,7 @@ def make_filter() -> None:
 
 if __name__ == "__main__":
     if "--filter" in sys.argv:
-        make_filter()
+        # --out DIR: where to write (a GPU host may only return some folders)
+        make_filter(sys.argv[sys.argv.index("--out") + 1] if "--out" in sys.argv else HERE)
     else:
         make_cpu()

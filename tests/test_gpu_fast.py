@@ -1,0 +1,98 @@
+"""GPU tests of the fast (chosen) form: BF16 filtered data, fast
+backprojection. Its error is stated in HU against the FP64 oracle, with the
+water level of the same geometry as the HU calibration (the reference's 3D
+weight scales the reconstructed level with the pitch)."""
+import numpy as np
+import pytest
+import torch
+
+from analyticalreconbigpatient_b200 import _lib, geometry as G, phantom as P
+from analyticalreconbigpatient_b200.pipeline import HelicalRecon, project
+from conftest import rel_l2
+from oracle_chain import hu_rmse, reference_slices
+
+pytestmark = pytest.mark.gpu
+
+HU_BUDGET = 1.0
+
+
+def recon(scan, fan, form):
+    rec = HelicalRecon(scan, form=form)
+    vol = rec.run(fan)
+    torch.cuda.synchronize()
+    out = vol.cpu().numpy()
+    rec.close()
+    return out
+
+
+def water_level(scan):
+    fan = project(scan, P.water_cylinder(radius=120.0, half_length=1e5))
+    v = recon(scan, fan, _lib.HR_FORM_PLAIN)
+    c = scan.XN // 2
+    r = max(2, int(40.0 / scan.dx))
+    return float(v[c - r: c + r, c - r: c + r, :].mean())
+
+
+@pytest.mark.parametrize("cfg", ["small", "full"])
+def test_fast_and_plain_hu_rmse_vs_fp64_oracle(cuda, cfg):
+    sc = G.config(cfg)
+    zlo = sc.h * sc.BetaS / (2 * np.pi)
+    zhi = sc.h * (sc.BetaS + sc.views * sc.dBeta) / (2 * np.pi)
+    obj = P.shepp_logan() if cfg == "small" else P.random_ellipsoids(1000, 60, (zlo, zhi))
+    fan = project(sc, obj)
+    fast = recon(sc, fan, _lib.HR_FORM_FAST)
+    plain = recon(sc, fan, _lib.HR_FORM_PLAIN)
+    wl = water_level(sc)
+    assert 0.8 * G.MU_WATER < wl < 1.05 * G.MU_WATER
+    fan_h = fan.cpu().numpy()
+    del fan
+    zis = [sc.ZN // 2] if cfg == "small" else [sc.ZN // 3, 2 * sc.ZN // 3]
+    ref, vox = reference_slices(sc, fan_h, zis, xy_step=1 if cfg == "small" else 2)
+    hu_fast = hu_rmse(fast.ravel()[vox], ref, wl)
+    hu_plain = hu_rmse(plain.ravel()[vox], ref, wl)
+    print(f"[{cfg}] HU RMSE vs FP64 oracle: fast {hu_fast:.4f}  plain {hu_plain:.5f}  "
+          f"(water level {wl:.6f}, {vox.size} voxels)")
+    assert hu_plain < 0.05
+    assert hu_fast < HU_BUDGET
+    assert rel_l2(plain.ravel()[vox], ref) < 1e-5
+
+
+def test_fast_backprojection_matches_plain_on_the_same_data(cuda):
+    """With identical BF16-representable filtered data the two backprojections
+    differ only by FP32 arithmetic and approximate SFU functions."""
+    from analyticalreconbigpatient_b200.pipeline import StagePlans
+
+    sc = G.Scan(ZL=16, pitch=0.9375, rotations=3, XN=64, YN=64, ZN=24, dx=4.0, dy=4.0, dz=1.0)
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(0)
+    filt = torch.tensor(rng.standard_normal((sc.PN, sc.ZL, sc.YL)).astype(np.float32), device=dev)
+    filt = filt.to(torch.bfloat16).to(torch.float32)  # make the data exactly BF16
+    plain = StagePlans(sc, _lib.HR_FORM_PLAIN)
+    fast = StagePlans(sc, _lib.HR_FORM_FAST)
+    pairs = torch.empty((sc.PN, sc.ZL, sc.YL), dtype=torch.int32, device=dev)
+    fast.pack(pairs, filt)
+    v1 = torch.empty((sc.YN, sc.XN, sc.ZN), dtype=torch.float32, device=dev)
+    v2 = torch.empty_like(v1)
+    plain.backproject(v1, filt)
+    fast.backproject(v2, pairs)
+    torch.cuda.synchronize()
+    a, b = v1.cpu().numpy(), v2.cpu().numpy()
+    plain.close()
+    fast.close()
+    assert rel_l2(b, a) < 2e-4
+    assert np.array_equal(a == 0, b == 0)
+
+
+def test_pack_pairs_layout(cuda):
+    dev = torch.device("cuda", 0)
+    x = torch.randn(7, 33, device=dev)
+    out = torch.empty((7, 33), dtype=torch.int32, device=dev)
+    _lib.check(_lib.load().hr_pack_bf16_pairs(out.data_ptr(), x.data_ptr(), 7, 33, 0))
+    torch.cuda.synchronize()
+    o = out.cpu().numpy().view(np.uint32)
+    lo = (o & 0xFFFF).astype(np.uint32) << 16
+    hi = o & 0xFFFF0000
+    xb = x.to(torch.bfloat16).to(torch.float32).cpu().numpy()
+    np.testing.assert_array_equal(lo.view(np.float32), xb)
+    np.testing.assert_array_equal(hi[:, :-1].view(np.float32), xb[:, 1:])
+    assert np.all(hi[:, -1] == 0)

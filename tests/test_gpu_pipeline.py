@@ -79,7 +79,7 @@ def test_water_cylinder_known_answer(cuda):
     ratio = core.mean() / G.MU_WATER
     assert 0.85 < ratio < 0.95
     # outside the body it is air
-    assert abs(vol[2:6, 2:6, :]).mean() < 0.02 * core.mean()
+    assert abs(vol[2:6, 2:6, :]).mean() < 0.05 * core.mean()
 
 
 def test_offcentre_sphere_lands_at_its_position(cuda):

@@ -34,7 +34,7 @@ def test_rebin_bit_exact_to_reference_golden(cuda, path):
 
 @pytest.mark.parametrize("ZL", [16, 6, 1])
 def test_rebin_bit_exact_small_config_and_odd_rows(cuda, ZL):
-    sc = G.config("small") if ZL == 16 else G.tiny(ZL=ZL, YL=200, iso_channel=100.75)
+    sc = G.config("small") if ZL == 16 else G.tiny(ZL=ZL, YL=200, det_pitch=1.0239 * 888 / 200, iso_channel=100.75)
     ra = sc.rebin_args()
     rng = np.random.default_rng(ZL)
     proj = rng.random((ra["ViewN"], ra["YL"], ra["ZL"]), dtype=np.float32)

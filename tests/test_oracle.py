@@ -160,3 +160,22 @@ def test_projector_ellipsoid_matches_sphere_formula():
     d = sc.SO * np.abs(np.sin(gam))
     expect = np.where(d < r, 2 * np.sqrt(np.maximum(r * r - d * d, 0)), 0)
     np.testing.assert_allclose(proj[0, :, 0], expect, rtol=1e-5, atol=1e-4)
+
+
+def test_windowed_oracle_chain_equals_full_chain():
+    """The helper that rebins/filters only the views a few slices need gives
+    the same FP64 result as the whole-scan chain."""
+    from oracle_chain import reference_slices
+
+    sc = G.Scan(ZL=8, pitch=0.9375, rotations=4, XN=12, YN=12, ZN=40, dx=16.0, dy=16.0, dz=0.8, YL=160,
+                det_pitch=1.0239 * 888 / 160, N_2pi=240, delta=15)
+    obj = P.random_ellipsoids(5, 6, (-10.0, 10.0), body=(120.0, 90.0), semi_axes=(10, 50))
+    fan = oracle.project_ellipsoids(obj, **P.projector_args(sc))
+    zis = [3, 20, 37]
+    vals, vox = reference_slices(sc, fan, zis)
+    reb = oracle.rebin_f64(fan, **sc.rebin_args())
+    rows = np.ascontiguousarray(reb.transpose(0, 2, 1)[sc.crop_front: sc.views - sc.crop_back])
+    filt = oracle.filter_f64(rows, **sc.filter_args())
+    w = oracle.weight_table(sc.N_2pi, sc.HSCoef, sc.delta)
+    full = oracle.bp_f64(filt, w, sc.bp_geom(), vox=vox)
+    assert rel_l2(vals, full) < 1e-10
