@@ -104,11 +104,12 @@ extern "C" int hr_filter_host(float* out, const float* in, int YL, int ZL, int V
   PlanGuard<hr_filter_plan, hr_filter_plan_destroy> plan;
   HR_TRY(hr_filter_plan_create(&plan.p, YL, ZL, ViewN, PLC, ZLC, dYL, dZL, SO));
   const size_t n = (size_t)YL * ZL * ViewN;
-  hr::DeviceBuffer dbuf;
-  HR_TRY(dbuf.alloc(n * sizeof(float)));
-  HR_CUDA_TRY(cudaMemcpy(dbuf.ptr, in, n * sizeof(float), cudaMemcpyHostToDevice));
-  HR_TRY(hr_filter_execute(plan.p, dbuf.as<float>(), dbuf.as<float>(), HR_LAYOUT_ROWS, 0, nullptr));
-  HR_CUDA_TRY(cudaMemcpy(out, dbuf.ptr, n * sizeof(float), cudaMemcpyDeviceToHost));
+  hr::DeviceBuffer din, dout;
+  HR_TRY(din.alloc(n * sizeof(float)));
+  HR_TRY(dout.alloc(n * sizeof(float)));
+  HR_CUDA_TRY(cudaMemcpy(din.ptr, in, n * sizeof(float), cudaMemcpyHostToDevice));
+  HR_TRY(hr_filter_execute(plan.p, dout.as<float>(), din.as<float>(), HR_LAYOUT_ROWS, 0, nullptr));
+  HR_CUDA_TRY(cudaMemcpy(out, dout.ptr, n * sizeof(float), cudaMemcpyDeviceToHost));
   return HR_OK;
 }
 

@@ -283,12 +283,16 @@ extern "C" int hr_filter_execute(const hr_filter_plan* p, float* d_out, const fl
   HR_REQUIRE(view0 >= 0, "hr_filter_execute: view0 < 0");
   HR_REQUIRE(in_layout == HR_LAYOUT_ROWS || in_layout == HR_LAYOUT_REBIN, "hr_filter_execute: unknown layout %d",
              in_layout);
+  // The kernel reads its input through the non-coherent read-only path
+  // (__restrict__), so input and output must not overlap.
+  const size_t in_views = (size_t)view0 + p->ViewN;
+  const char* ib = reinterpret_cast<const char*>(d_in);
+  const char* ie = ib + in_views * p->ZL * p->YL * sizeof(float);
+  const char* ob = reinterpret_cast<const char*>(d_out);
+  const char* oe = ob + (size_t)p->ViewN * p->ZL * p->YL * sizeof(float);
+  HR_REQUIRE(oe <= ib || ie <= ob, "hr_filter_execute: input and output overlap (in-place filtering is not supported)");
   cudaStream_t s = hr::as_stream(stream);
-  if (in_layout == HR_LAYOUT_ROWS) {
-    HR_REQUIRE(d_out != d_in || view0 == 0, "hr_filter_execute: in-place needs view0 == 0");
-    return launch_layout<HR_LAYOUT_ROWS>(p, d_out, d_in, view0, s);
-  }
-  HR_REQUIRE(d_out != d_in, "hr_filter_execute: the rebin layout cannot be filtered in place");
+  if (in_layout == HR_LAYOUT_ROWS) return launch_layout<HR_LAYOUT_ROWS>(p, d_out, d_in, view0, s);
   return launch_layout<HR_LAYOUT_REBIN>(p, d_out, d_in, view0, s);
 }
 

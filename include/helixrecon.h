@@ -144,7 +144,8 @@ typedef struct hr_filter_plan hr_filter_plan;
 int hr_filter_plan_create(hr_filter_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC, float dYL,
                           float dZL, float SO);
 /* Filters views [view0, view0+ViewN) of d_in (laid out as in_layout, holding
- * at least view0+ViewN views) into d_out [ViewN][ZL][YL]. */
+ * at least view0+ViewN views) into d_out [ViewN][ZL][YL]. d_in and d_out must
+ * not overlap (HR_ERR_INVALID_ARGUMENT otherwise). */
 int hr_filter_execute(const hr_filter_plan* plan, float* d_out, const float* d_in, int in_layout, int view0,
                       void* stream);
 void hr_filter_plan_destroy(hr_filter_plan* plan);

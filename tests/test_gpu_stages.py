@@ -49,8 +49,9 @@ def test_filter_vs_reference_cufft_golden(cuda, path):
     d = np.load(path)
     YL, ZL, ViewN = (int(v) for v in d["sizes"])
     PLC, ZLC, dYL, dZL, SO = (float(v) for v in d["args"])
-    mine = np.empty_like(d["proj"])
-    _lib.load().filtering(mine.ctypes.data, d["proj"].ctypes.data, YL, ZL, ViewN, PLC, ZLC, dYL, dZL, SO)
+    proj = d["proj"]  # keep the array alive across the C call
+    mine = np.empty_like(proj)
+    _lib.load().filtering(mine.ctypes.data, proj.ctypes.data, YL, ZL, ViewN, PLC, ZLC, dYL, dZL, SO)
     assert rel_l2(mine, d["out"]) < PLAIN_TOL
 
 
@@ -148,3 +149,21 @@ def test_errors_are_raised_not_swallowed(cuda):
         api.reWeigAdFiltr_GPU(np.zeros((2, 2, 3000), np.float32), 0, 0, 1, 1, 541)
     with pytest.raises(ValueError):
         api.ParallelRebinningCBCurve(np.zeros(10, np.float32), 8, 4, 10, 1, 0.01, 0.1, 1, 1, 0.1, 541, 1)
+
+
+def test_filter_refuses_overlapping_buffers(cuda):
+    import torch
+
+    sc = G.tiny(YL=64, ZL=4)
+    fa = sc.filter_args()
+    plan = ctypes.c_void_p()
+    lib = _lib.load()
+    _lib.check(lib.hr_filter_plan_create(ctypes.byref(plan), fa["YL"], fa["ZL"], 10, fa["PLC"], fa["ZLC"], fa["dYL"],
+                                         fa["dZL"], fa["SO"]))
+    x = torch.zeros((11, fa["ZL"], fa["YL"]), device=cuda)
+    assert lib.hr_filter_execute(plan, x.data_ptr(), x.data_ptr(), 0, 0, 0) == 1
+    assert lib.hr_filter_execute(plan, x[1:].data_ptr(), x.data_ptr(), 0, 0, 0) == 1
+    y = torch.zeros_like(x)
+    assert lib.hr_filter_execute(plan, y.data_ptr(), x.data_ptr(), 0, 1, 0) == 0
+    torch.cuda.synchronize()
+    lib.hr_filter_plan_destroy(plan)
