@@ -74,6 +74,7 @@ _SIGS = {
     "hr_bp_plan_destroy": (None, [_p]),
     "hr_project_ellipsoids": (_i, [_p, _i, _i, _i] + [_d] * 9 + [_p, _i, _p]),
     "hr_pack_bf16_pairs": (_i, [_p, _p, ctypes.c_longlong, _i, _p]),
+    "hr_bp_plain_noalloc": (_i, [_p, _p, _p, ctypes.POINTER(BpGeom), _p]),
     "hr_recon_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc)]),
     "hr_recon_execute": (_i, [_p, _p, _p, _p]),
     "hr_recon_execute_host": (_i, [_p, _p, _p]),

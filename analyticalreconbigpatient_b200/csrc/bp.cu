@@ -363,3 +363,102 @@ extern "C" void hr_bp_plan_destroy(hr_bp_plan* pl) {
   cudaFree(pl->d_wd);
   delete pl;
 }
+
+// ---------------------------------------------------------------------------
+// Plain-form backprojection that allocates nothing.
+//
+// Some callers cannot call cudaMalloc: code that runs while its stream is being
+// captured into a CUDA graph (allocation is not allowed during capture),
+// streaming pipelines that must not allocate after start-up because
+// cudaMalloc/cudaFree synchronise the device, and hosts such as MATLAB or a
+// framework's pooling allocator that own all device memory. This entry keeps
+// its only scratch -- the per-view cos/sin/source-height table -- in a
+// file-scope device array of kNoAllocMaxViews entries (768 KiB, held by every
+// GPU that loads the library until the process exits) and takes everything
+// else (filtered data, weight table, volume) from the caller.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+constexpr int kNoAllocMaxViews = 32768;
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) ViewTab g_noalloc_views[kNoAllocMaxViews];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+ViewTab* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_views on the current device, looked up once per
+// device (with that device current). In host code the array's name is only a
+// host-side stand-in, never a device address.
+int noalloc_views(ViewTab** out) {
+  int dev = 0;
+  HR_CUDA_TRY(cudaGetDevice(&dev));
+  HR_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, "hr_bp_plain_noalloc: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    HR_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_views));
+    g_noalloc_ptr[dev] = static_cast<ViewTab*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return HR_OK;
+}
+
+// cos/sin/h*View/2pi of every view, with the same double expressions the plan
+// evaluates on the host (View = BetaS + p*DeltaFai, h*View*invPI).
+__global__ void noalloc_view_table_kernel(ViewTab* __restrict__ tab, int PN, double BetaS, double DeltaFai,
+                                          double h) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < PN; p += gridDim.x * blockDim.x) {
+    const double View = __dadd_rn(BetaS, __dmul_rn((double)p, DeltaFai));
+    double s, c;
+    sincos(View, &s, &c);
+    tab[p] = ViewTab{c, s, __dmul_rn(__dmul_rn(h, View), kInvTwoPi)};
+  }
+}
+
+}  // namespace
+
+extern "C" int hr_bp_plain_noalloc(float* d_vol, const float* d_fp, const float* d_w, const hr_bp_geom* g,
+                                   void* stream) {
+  hr::clear_error();
+  HR_REQUIRE(d_vol != nullptr && d_fp != nullptr && d_w != nullptr && g != nullptr,
+             "hr_bp_plain_noalloc: NULL argument");
+  HR_REQUIRE(g->XN > 0 && g->YN > 0 && g->ZN > 0 && g->YL > 1 && g->ZL > 1 && g->PN > 0 && g->N_2pi > 1,
+             "hr_bp_plain_noalloc: invalid sizes");
+  HR_REQUIRE(g->PN <= kNoAllocMaxViews,
+             "hr_bp_plain_noalloc: PN=%d views exceed the fixed scratch table of %d views (use hr_bp_plan_create)",
+             g->PN, kNoAllocMaxViews);
+  HR_REQUIRE(g->N_2pi <= 8192, "hr_bp_plain_noalloc: N_2pi=%d exceeds 8192", g->N_2pi);
+  HR_REQUIRE(g->h != 0.0 && g->DeltaFai != 0.0 && g->dYL != 0.0 && g->dZL != 0.0 && g->SO > 0.0,
+             "hr_bp_plain_noalloc: h, DeltaFai, dYL, dZL must be non-zero and SO > 0");
+  const int half = (int)std::ceil(g->N_pi * g->HSCoef);
+  HR_REQUIRE(half >= 0 && (double)half <= g->N_pi && g->N_pi + half <= g->N_2pi - 1 &&
+                 2.0 * g->N_pi <= g->N_2pi + 1e-9,
+             "hr_bp_plain_noalloc: HSCoef=%g, N_pi=%g give a view window outside the weight table", g->HSCoef,
+             g->N_pi);
+  BpParams P{};
+  P.XN = g->XN; P.YN = g->YN; P.ZN = g->ZN; P.YL = g->YL; P.ZL = g->ZL; P.PN = g->PN; P.N_2pi = g->N_2pi;
+  P.half = half;
+  P.XNC = g->XNC; P.YNC = g->YNC; P.ZNC = g->ZNC; P.dx = g->dx; P.dy = g->dy; P.dz = g->dz;
+  P.YLC = g->YLC; P.ZLC = g->ZLC; P.dYL = g->dYL; P.dZL = g->dZL; P.h = g->h; P.BetaS = g->BetaS;
+  P.DeltaFai = g->DeltaFai; P.N_pi = g->N_pi; P.SO = g->SO; P.SD = g->SD; P.k1 = g->k1;
+  P.SO2 = g->SO * g->SO;
+  P.SOSD = g->SO * g->SD;
+  P.SOSDdZL = P.SOSD / g->dZL;
+  P.k1f = (float)g->k1;
+  P.DeltaFaif = (float)g->DeltaFai;
+  dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, (P.ZN + kNzPlain - 1) / kNzPlain);
+  HR_REQUIRE(grid.z <= 65535 && grid.y <= 65535, "hr_bp_plain_noalloc: grid too large");
+  ViewTab* views = nullptr;
+  HR_TRY(noalloc_views(&views));
+  cudaStream_t s = hr::as_stream(stream);
+  noalloc_view_table_kernel<<<(P.PN + 255) / 256, 256, 0, s>>>(views, P.PN, P.BetaS, P.DeltaFai, P.h);
+  HR_CUDA_TRY(cudaGetLastError());
+  bp_plain_kernel<kNzPlain><<<grid, dim3(kBx, kBy), sizeof(float) * P.N_2pi, s>>>(d_vol, d_fp, views, d_w, P);
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}

@@ -167,6 +167,20 @@ int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const double* w, i
 int hr_bp_execute(const hr_bp_plan* plan, void* d_vol, const void* d_fp, void* stream);
 void hr_bp_plan_destroy(hr_bp_plan* plan);
 
+/* ---- backprojection that allocates nothing ------------------------------ */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc:
+ * code running while its stream is captured into a CUDA graph, streaming
+ * pipelines that may not allocate after start-up (cudaMalloc/cudaFree
+ * synchronise the device), and hosts whose pooling allocator owns all device
+ * memory. Same result as a HR_FORM_PLAIN plan: d_vol [YN][XN][ZN] float,
+ * d_fp [PN][ZL][YL] float, d_w the N_2pi view weights as float on the device.
+ * Its per-view table lives in a fixed device array inside the library, so
+ * PN is limited to 32768 views (HR_ERR_INVALID_ARGUMENT beyond). The first
+ * call on a device looks up that array's address (cudaGetSymbolAddress) and
+ * should come before any stream capture. All calls share the array: calls
+ * that overlap on the GPU (other streams, other threads) race. */
+int hr_bp_plain_noalloc(float* d_vol, const float* d_fp, const float* d_w, const hr_bp_geom* g, void* stream);
+
 /* ---- BF16 channel pairs (the fast form's filtered-data layout) ---------- */
 /* d_out[r][u] = bf16(d_in[r][u]) | bf16(d_in[r][u+1]) << 16 (round to nearest
  * even; channel YL pairs with 0), for rows r in [0, rows). The fast form's
