@@ -74,6 +74,12 @@ _SIGS = {
     "hr_bp_plan_destroy": (None, [_p]),
     "hr_project_ellipsoids": (_i, [_p, _i, _i, _i] + [_d] * 9 + [_p, _i, _p]),
     "hr_pack_bf16_pairs": (_i, [_p, _p, ctypes.c_longlong, _i, _p]),
+    "hr_filter_tc_plan_create": (_i, [ctypes.POINTER(_p), _i, _i, _i] + [_f] * 5),
+    "hr_filter_tc_execute": (_i, [_p, _p, _p, _i, _i, _p]),
+    "hr_filter_tc_check": (_i, [_p]),
+    "hr_filter_tc_device_bytes": (ctypes.c_size_t, [_p]),
+    "hr_filter_tc_plan_destroy": (None, [_p]),
+    "hr_recon_check": (_i, [_p]),
     "hr_bp_plain_noalloc": (_i, [_p, _p, _p, ctypes.POINTER(BpGeom), _p]),
     "hr_recon_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc)]),
     "hr_recon_execute": (_i, [_p, _p, _p, _p]),

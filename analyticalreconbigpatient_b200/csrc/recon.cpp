@@ -15,7 +15,8 @@
 struct hr_recon_plan {
   hr_recon_desc d;
   hr_rebin_plan* rebin = nullptr;
-  hr_filter_plan* filter = nullptr;
+  hr_filter_plan* filter = nullptr;        // plain form: FFT filter
+  hr_filter_tc_plan* filter_tc = nullptr;  // fast form: tensor-core Toeplitz filter
   hr_bp_plan* bp = nullptr;
   float* d_rebinned = nullptr;  // [ViewN][YL][ZL]
   float* d_filtered = nullptr;  // [PN][ZL][YL]
@@ -32,6 +33,7 @@ void destroy(hr_recon_plan* p) {
   if (!p) return;
   hr_rebin_plan_destroy(p->rebin);
   hr_filter_plan_destroy(p->filter);
+  hr_filter_tc_plan_destroy(p->filter_tc);
   hr_bp_plan_destroy(p->bp);
   cudaFree(p->d_rebinned);
   cudaFree(p->d_filtered);
@@ -66,15 +68,18 @@ extern "C" int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* d
   p->d.w = nullptr;
   int st = hr_rebin_plan_create(&p->rebin, d->YL, d->ZL, d->ViewN, d->YLC, d->dYA, d->DeltaTheta, d->PLC, d->DeltaT,
                                 d->DeltaFai, d->SO);
-  if (st == HR_OK)
+  const bool fast = d->form == HR_FORM_FAST;
+  if (st == HR_OK && fast)
+    st = hr_filter_tc_plan_create(&p->filter_tc, d->YL, d->ZL, d->bp.PN, d->fPLC, d->fZLC, d->fdYL, d->fdZL, d->fSO);
+  if (st == HR_OK && !fast)
     st = hr_filter_plan_create(&p->filter, d->YL, d->ZL, d->bp.PN, d->fPLC, d->fZLC, d->fdYL, d->fdZL, d->fSO);
   if (st == HR_OK) st = hr_bp_plan_create(&p->bp, &d->bp, d->w, d->form);
   const size_t nfan = (size_t)d->YL * d->ZL * d->ViewN;
   const size_t nfilt = (size_t)d->YL * d->ZL * d->bp.PN;
   const size_t nvol = (size_t)d->bp.XN * d->bp.YN * d->bp.ZN;
   if (st == HR_OK) st = alloc(p, (void**)&p->d_rebinned, nfan * sizeof(float));
-  if (st == HR_OK) st = alloc(p, (void**)&p->d_filtered, nfilt * sizeof(float));
-  if (st == HR_OK && d->form == HR_FORM_FAST) st = alloc(p, (void**)&p->d_pairs, nfilt * sizeof(uint32_t));
+  if (st == HR_OK && !fast) st = alloc(p, (void**)&p->d_filtered, nfilt * sizeof(float));
+  if (st == HR_OK && fast) st = alloc(p, (void**)&p->d_pairs, nfilt * sizeof(uint32_t));
   if (st == HR_OK) st = alloc(p, (void**)&p->d_fan, nfan * sizeof(float));
   if (st == HR_OK) st = alloc(p, (void**)&p->d_vol, nvol * sizeof(float));
   if (st == HR_OK) {
@@ -92,12 +97,11 @@ extern "C" int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* d
 extern "C" int hr_recon_execute(const hr_recon_plan* p, float* d_vol, const float* d_fan, void* stream) {
   HR_REQUIRE(p != nullptr && d_vol != nullptr && d_fan != nullptr, "hr_recon_execute: NULL argument");
   HR_TRY(hr_rebin_execute(p->rebin, p->d_rebinned, d_fan, stream));
-  HR_TRY(hr_filter_execute(p->filter, p->d_filtered, p->d_rebinned, HR_LAYOUT_REBIN, p->d.view0, stream));
   if (p->d.form == HR_FORM_FAST) {
-    HR_TRY(hr::pack_pairs(p->d_pairs, p->d_filtered, (long long)p->d.ZL * p->d.bp.PN, p->d.YL,
-                          hr::as_stream(stream)));
+    HR_TRY(hr_filter_tc_execute(p->filter_tc, p->d_pairs, p->d_rebinned, HR_LAYOUT_REBIN, p->d.view0, stream));
     return hr_bp_execute(p->bp, d_vol, p->d_pairs, stream);
   }
+  HR_TRY(hr_filter_execute(p->filter, p->d_filtered, p->d_rebinned, HR_LAYOUT_REBIN, p->d.view0, stream));
   return hr_bp_execute(p->bp, d_vol, p->d_filtered, stream);
 }
 
@@ -113,6 +117,14 @@ extern "C" int hr_recon_execute_host(hr_recon_plan* p, float* h_vol, const float
   return HR_OK;
 }
 
-extern "C" size_t hr_recon_device_bytes(const hr_recon_plan* p) { return p ? p->bytes : 0; }
+extern "C" int hr_recon_check(const hr_recon_plan* p) {
+  HR_REQUIRE(p != nullptr, "hr_recon_check: NULL plan");
+  if (p->filter_tc) return hr_filter_tc_check(p->filter_tc);
+  return HR_OK;
+}
+
+extern "C" size_t hr_recon_device_bytes(const hr_recon_plan* p) {
+  return p ? p->bytes + (p->filter_tc ? hr_filter_tc_device_bytes(p->filter_tc) : 0) : 0;
+}
 
 extern "C" void hr_recon_plan_destroy(hr_recon_plan* p) { destroy(p); }

@@ -64,6 +64,10 @@ class HelicalRecon:
     def device_bytes(self) -> int:
         return int(_lib.load().hr_recon_device_bytes(self._plan))
 
+    def check(self) -> None:
+        """Raise if a kernel of an earlier execution reported a timed-out pipeline wait (synchronises)."""
+        _lib.check(_lib.load().hr_recon_check(self._plan))
+
     def run(self, fan: torch.Tensor, volume: torch.Tensor | None = None, stream=None) -> torch.Tensor:
         """fan: device float32 [views][YL][ZL] (post-flip channel order)."""
         vol = self.volume if volume is None else volume
@@ -112,6 +116,10 @@ class StagePlans:
         self.w = view_weights(scan)
         geom = _lib.BpGeom.from_dict(scan.bp_geom())
         _lib.check(lib.hr_bp_plan_create(ctypes.byref(self._bp), ctypes.byref(geom), self.w.ctypes.data, form))
+        self._filter_tc = ctypes.c_void_p()
+        if form == _lib.HR_FORM_FAST:
+            _lib.check(lib.hr_filter_tc_plan_create(ctypes.byref(self._filter_tc), fa["YL"], fa["ZL"], fa["ViewN"],
+                                                    fa["PLC"], fa["ZLC"], fa["dYL"], fa["dZL"], fa["SO"]))
 
     def rebin(self, out: torch.Tensor, fan: torch.Tensor, stream: int = 0) -> None:
         _lib.check(_lib.load().hr_rebin_execute(self._rebin, out.data_ptr(), fan.data_ptr(), stream))
@@ -123,6 +131,15 @@ class StagePlans:
     def backproject(self, vol: torch.Tensor, fp: torch.Tensor, stream: int = 0) -> None:
         _lib.check(_lib.load().hr_bp_execute(self._bp, vol.data_ptr(), fp.data_ptr(), stream))
 
+    def filter_tc(self, pairs: torch.Tensor, inp: torch.Tensor, in_layout: int, view0: int, stream: int = 0) -> None:
+        """Tensor-core Toeplitz filter straight to BF16 channel pairs (fast form)."""
+        _lib.check(_lib.load().hr_filter_tc_execute(self._filter_tc, pairs.data_ptr(), inp.data_ptr(), in_layout,
+                                                    view0, stream))
+
+    def check(self) -> None:
+        if self._filter_tc:
+            _lib.check(_lib.load().hr_filter_tc_check(self._filter_tc))
+
     def pack(self, out: torch.Tensor, filtered: torch.Tensor, stream: int = 0) -> None:
         """FP32 filtered rows -> BF16 channel pairs (the fast form's layout)."""
         s = self.scan
@@ -131,8 +148,8 @@ class StagePlans:
     def close(self) -> None:
         lib = _lib.load()
         for attr, fn in (("_rebin", lib.hr_rebin_plan_destroy), ("_filter", lib.hr_filter_plan_destroy),
-                         ("_bp", lib.hr_bp_plan_destroy)):
-            if getattr(self, attr):
+                         ("_bp", lib.hr_bp_plan_destroy), ("_filter_tc", lib.hr_filter_tc_plan_destroy)):
+            if getattr(self, attr, None):
                 fn(getattr(self, attr))
                 setattr(self, attr, ctypes.c_void_p())
 

@@ -248,27 +248,28 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
     # ---- per-stage timing (warm) ---------------------------------------------
     stages = StagePlans(scan, form)
     rebinned = torch.empty((scan.views, scan.YL, scan.ZL), dtype=torch.float32, device=dev)
-    filtered = torch.empty((scan.PN, scan.ZL, scan.YL), dtype=torch.float32, device=dev)
+    filtered = None if fast else torch.empty((scan.PN, scan.ZL, scan.YL), dtype=torch.float32, device=dev)
     pairs = torch.empty((scan.PN, scan.ZL, scan.YL), dtype=torch.int32, device=dev) if fast else None
     vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, device=dev)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-    names = ["rebin", "filter", "pack", "backprojection"]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    names = ["rebin", "filter", "backprojection"]
     stage_ms = {k: [] for k in names}
     for i in range(args.warmup + args.steps):
         ev[0].record(stream)
         stages.rebin(rebinned, fan, st)
         ev[1].record(stream)
-        stages.filter(filtered, rebinned, _lib.HR_LAYOUT_REBIN, scan.crop_front, st)
+        if fast:  # tensor-core Toeplitz filter straight to BF16 channel pairs
+            stages.filter_tc(pairs, rebinned, _lib.HR_LAYOUT_REBIN, scan.crop_front, st)
+        else:
+            stages.filter(filtered, rebinned, _lib.HR_LAYOUT_REBIN, scan.crop_front, st)
         ev[2].record(stream)
-        if fast:
-            stages.pack(pairs, filtered, st)
-        ev[3].record(stream)
         stages.backproject(vol, pairs if fast else filtered, st)
-        ev[4].record(stream)
+        ev[3].record(stream)
         stream.synchronize()
         if i >= args.warmup:
-            for k in range(4):
+            for k in range(3):
                 stage_ms[names[k]].append(ev[k].elapsed_time(ev[k + 1]))
+    stages.check()
     del rebinned, filtered, pairs, vol
     stages.close()
     torch.cuda.empty_cache()
@@ -293,6 +294,7 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
         tm = torch.tensor([ms], device=dev)
         dist.all_reduce(tm, op=dist.ReduceOp.MAX)
         ms = float(tm.item())
+    rec.check()
     out = {"ms_per_step": ms, "stages_ms": {k: statistics.mean(v) for k, v in stage_ms.items() if v},
            "launches_per_step": 4 if fast else 3}
 

@@ -150,6 +150,23 @@ int hr_filter_execute(const hr_filter_plan* plan, float* d_out, const float* d_i
                       void* stream);
 void hr_filter_plan_destroy(hr_filter_plan* plan);
 
+/* ---- tensor-core filter plan (fast form) -------------------------------- */
+/* Preweight + ramp filter as a split-BF16 Toeplitz matrix product on the
+ * tcgen05 tensor cores (FP32 accumulation in TMEM); writes the fast
+ * backprojection's BF16 channel pairs [ViewN][ZL][YL] (uint32). Needs an
+ * sm_100 device. The plan holds the split operands (4 bytes per sample of
+ * workspace plus the Toeplitz matrix). */
+typedef struct hr_filter_tc_plan hr_filter_tc_plan;
+int hr_filter_tc_plan_create(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC, float dYL,
+                             float dZL, float SO);
+int hr_filter_tc_execute(const hr_filter_tc_plan* plan, uint32_t* d_pairs, const float* d_in, int in_layout,
+                         int view0, void* stream);
+/* Reads the plan's device error flag (synchronous): HR_ERR_CUDA if a kernel
+ * pipeline wait timed out in an earlier execution. */
+int hr_filter_tc_check(const hr_filter_tc_plan* plan);
+size_t hr_filter_tc_device_bytes(const hr_filter_tc_plan* plan);
+void hr_filter_tc_plan_destroy(hr_filter_tc_plan* plan);
+
 /* ---- backprojection plan ------------------------------------------------ */
 typedef struct hr_bp_geom {
   int N_2pi, XN, YN, ZN, YL, ZL, PN;
@@ -211,6 +228,8 @@ int hr_recon_execute(const hr_recon_plan* plan, float* d_vol, const float* d_fan
 /* Host pointers (pinned for full copy speed): copies the fan data in, runs the
  * chain, copies the volume out; returns when h_vol is written. */
 int hr_recon_execute_host(hr_recon_plan* plan, float* h_vol, const float* h_fan);
+/* Synchronous health check of the plan's kernels (tensor-core filter flag). */
+int hr_recon_check(const hr_recon_plan* plan);
 /* Device bytes the plan holds (tables + intermediate + host-staging buffers). */
 size_t hr_recon_device_bytes(const hr_recon_plan* plan);
 void hr_recon_plan_destroy(hr_recon_plan* plan);
