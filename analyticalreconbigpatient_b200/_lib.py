@@ -80,6 +80,10 @@ _SIGS = {
     "hr_filter_tc_device_bytes": (ctypes.c_size_t, [_p]),
     "hr_filter_tc_plan_destroy": (None, [_p]),
     "hr_recon_check": (_i, [_p]),
+    "hr_recon_describe": (_i, [_p, ctypes.c_char_p, _i]),
+    "hr_bp_autotune": (_i, [_p, _p, _p, _p]),
+    "hr_bp_describe": (_i, [_p, ctypes.c_char_p, _i]),
+    "hr_bp_select": (_i, [_p, _i]),
     "hr_bp_plain_noalloc": (_i, [_p, _p, _p, ctypes.POINTER(BpGeom), _p]),
     "hr_recon_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc)]),
     "hr_recon_execute": (_i, [_p, _p, _p, _p]),

@@ -355,6 +355,32 @@ extern "C" int hr_bp_execute(const hr_bp_plan* pl, void* d_vol, const void* d_fp
   return HR_OK;
 }
 
+extern "C" int hr_bp_autotune(hr_bp_plan* pl, void* d_vol, const void* d_fp, void* stream) {
+  HR_REQUIRE(pl != nullptr && d_vol != nullptr && d_fp != nullptr, "hr_bp_autotune: NULL argument");
+  if (pl->form != HR_FORM_FAST) return HR_OK;
+  return hr::bp_fast_autotune(&pl->fast, pl->fg, static_cast<float*>(d_vol), static_cast<const uint32_t*>(d_fp),
+                              hr::as_stream(stream));
+}
+
+extern "C" int hr_bp_select(hr_bp_plan* pl, int variant) {
+  HR_REQUIRE(pl != nullptr, "hr_bp_select: NULL plan");
+  if (pl->form != HR_FORM_FAST) return variant == 0 ? HR_OK : hr::fail(HR_ERR_INVALID_ARGUMENT, "hr_bp_select: "
+                                                                        "only the fast form has variants");
+  HR_REQUIRE(variant >= 0 && variant < hr::kFastVariants_n, "hr_bp_select: variant %d out of range [0, %d)",
+             variant, hr::kFastVariants_n);
+  pl->fast.variant = variant;
+  return HR_OK;
+}
+
+extern "C" int hr_bp_describe(const hr_bp_plan* pl, char* buf, int len) {
+  HR_REQUIRE(pl != nullptr, "hr_bp_describe: NULL plan");
+  if (pl->form == HR_FORM_FAST) return hr::bp_fast_describe(pl->fast, buf, len);
+  if (buf && len > 0)
+    snprintf(buf, (size_t)len, "%s slices_per_thread=%d tile=%dx%d", pl->form == HR_FORM_FP64 ? "fp64" : "plain",
+             pl->form == HR_FORM_FP64 ? kNzFp64 : kNzPlain, kBx, kBy);
+  return HR_OK;
+}
+
 extern "C" void hr_bp_plan_destroy(hr_bp_plan* pl) {
   if (!pl) return;
   hr::bp_fast_destroy(&pl->fast);

@@ -67,16 +67,50 @@ struct FastParams {
   float XNC, YNC, dx, dy, SO2, SOSDdZL, invdYL, YLC0, ZLC0, k1, DeltaFai;
 };
 
-template <int NZ>
+// Per (column, view) quantities shared by the slices of a thread.
+struct ColView {
+  float K, C, fu;
+  int u0;
+};
+
+__device__ __forceinline__ bool col_view(const FastParams& P, float x, float y, float2 cs, ColView& cv) {
+  const float UU = -x * cs.x - y * cs.y;
+  const float Yr = -x * cs.y + y * cs.x;
+  const float t1sq = P.SO2 - Yr * Yr;
+  const float temp1 = t1sq * rsqrtf(t1sq);
+  const float A = temp1 + UU, B = temp1 - UU;
+  cv.K = P.SOSDdZL * rcp_approx(temp1 * A);
+  cv.C = P.k1 * lg2_approx(B * rcp_approx(A));
+  const float u1 = fmaf(Yr, P.invdYL, P.YLC0);
+  float u0f;
+  cv.u0 = floor_magic(u1, u0f);
+  cv.fu = u1 - u0f;
+  return (unsigned)cv.u0 <= (unsigned)(P.YL - 2);
+}
+
+__device__ __forceinline__ float blend(uint32_t w0, uint32_t w1, float fu, float fz) {
+  const float a0 = __uint_as_float(w0 << 16), a1 = __uint_as_float(w0 & 0xffff0000u);
+  const float b0 = __uint_as_float(w1 << 16), b1 = __uint_as_float(w1 & 0xffff0000u);
+  const float ra = fmaf(fu, a1 - a0, a0);
+  const float rb = fmaf(fu, b1 - b0, b0);
+  return fmaf(fz, rb - ra, ra);
+}
+
+// NZ slices per thread; CH == 0: slices one after the other (branch per
+// slice); CH > 0: chunks of CH slices whose row positions are computed first,
+// whose 2*CH gathers are then issued together (addresses clamped into the
+// detector, out-of-detector or out-of-window slices weighted by 0), and only
+// then consumed -- more loads in flight per warp at the cost of registers.
+template <int NZ, int CH>
 __global__ void __launch_bounds__(kBx* kBy) bp_fast_kernel(float* __restrict__ vol, const uint32_t* __restrict__ fpb,
                                                           const float2* __restrict__ trig,
                                                           const float2* __restrict__ ztab,
                                                           const uint32_t* __restrict__ zmask,
                                                           const int2* __restrict__ zblock,
-                                                          const int* __restrict__ zoff, FastParams P) {
+                                                          const int* __restrict__ zoff, FastParams P, int b_first) {
   const int xi = blockIdx.x * kBx + threadIdx.x;
   const int yi = blockIdx.y * kBy + threadIdx.y;
-  const int b = blockIdx.z;
+  const int b = b_first + blockIdx.z;
   const int z0 = b * NZ;
   if (xi >= P.XN || yi >= P.YN) return;
   const int2 blk = zblock[b];  // {first view, number of views} of the block's union window
@@ -93,44 +127,177 @@ __global__ void __launch_bounds__(kBx* kBy) bp_fast_kernel(float* __restrict__ v
     const uint32_t mask = __ldg(bmask + q);
     if (mask == 0u) continue;
     const int p = blk.x + q;
-    const float2 cs = __ldg(trig + p);
-    const float UU = -x * cs.x - y * cs.y;
-    const float Yr = -x * cs.y + y * cs.x;
-    const float t1sq = P.SO2 - Yr * Yr;
-    const float temp1 = t1sq * rsqrtf(t1sq);
-    const float A = temp1 + UU, B = temp1 - UU;
-    const float K = P.SOSDdZL * rcp_approx(temp1 * A);
-    const float C = P.k1 * lg2_approx(B * rcp_approx(A));
-    float u0f;
-    const int u0 = floor_magic(fmaf(Yr, P.invdYL, P.YLC0), u0f);
-    if ((unsigned)u0 > (unsigned)(P.YL - 2)) continue;
-    const float fu = fmaf(Yr, P.invdYL, P.YLC0) - u0f;
-    const uint32_t* col = fpb + (size_t)p * plane + u0;
+    ColView cv;
+    if (!col_view(P, x, y, __ldg(trig + p), cv)) continue;
+    const uint32_t* col = fpb + (size_t)p * plane + cv.u0;
     const float2* e = btab + (size_t)q * NZ;
+    if constexpr (CH == 0) {
 #pragma unroll
-    for (int m = 0; m < NZ; ++m) {
-      if (!(mask & (1u << m))) continue;
-      const float2 tq = __ldg(e + m);  // {t2, Q}
-      float v0f;
-      const float v1 = fmaf(tq.x, K, P.ZLC0);
-      const int v0 = floor_magic(v1, v0f);
-      if ((unsigned)v0 > (unsigned)(P.ZL - 2)) continue;
-      const float fz = v1 - v0f;
-      const uint32_t w0 = __ldg(col + (size_t)v0 * P.YL);
-      const uint32_t w1 = __ldg(col + (size_t)(v0 + 1) * P.YL);
-      const float a0 = __uint_as_float(w0 << 16), a1 = __uint_as_float(w0 & 0xffff0000u);
-      const float b0 = __uint_as_float(w1 << 16), b1 = __uint_as_float(w1 & 0xffff0000u);
-      const float ra = fmaf(fu, a1 - a0, a0);
-      const float rb = fmaf(fu, b1 - b0, b0);
-      const float tap = fmaf(fz, rb - ra, ra);
-      const float wgt = rcp_approx(1.0f + ex2_approx(tq.y + C));
-      res[m] = fmaf(wgt, tap, res[m]);
+      for (int m = 0; m < NZ; ++m) {
+        if (!(mask & (1u << m))) continue;
+        const float2 tq = __ldg(e + m);  // {t2, Q}
+        float v0f;
+        const float v1 = fmaf(tq.x, cv.K, P.ZLC0);
+        const int v0 = floor_magic(v1, v0f);
+        if ((unsigned)v0 > (unsigned)(P.ZL - 2)) continue;
+        const uint32_t w0 = __ldg(col + (size_t)v0 * P.YL);
+        const uint32_t w1 = __ldg(col + (size_t)(v0 + 1) * P.YL);
+        const float wgt = rcp_approx(1.0f + ex2_approx(tq.y + cv.C));
+        res[m] = fmaf(wgt, blend(w0, w1, cv.fu, v1 - v0f), res[m]);
+      }
+    } else {
+      const float4* e4 = reinterpret_cast<const float4*>(e);
+#pragma unroll
+      for (int c = 0; c < NZ / CH; ++c) {
+        const uint32_t cm = (mask >> (c * CH)) & ((1u << CH) - 1u);
+        if (cm == 0u) continue;  // uniform over the CTA
+        float t2[CH], qv[CH], fz[CH];
+        int vrow[CH];
+        bool ok[CH];
+#pragma unroll
+        for (int i = 0; i < CH; i += 2) {
+          const float4 t = __ldg(e4 + (c * CH + i) / 2);  // {t2, Q} of two slices
+          t2[i] = t.x; qv[i] = t.y; t2[i + 1] = t.z; qv[i + 1] = t.w;
+        }
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+          float v0f;
+          const float v1 = fmaf(t2[i], cv.K, P.ZLC0);
+          const int v0 = floor_magic(v1, v0f);
+          ok[i] = ((cm >> i) & 1u) && (unsigned)v0 <= (unsigned)(P.ZL - 2);
+          vrow[i] = ok[i] ? v0 : 0;
+          fz[i] = v1 - v0f;
+        }
+        uint32_t w0[CH], w1[CH];
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+          w0[i] = __ldg(col + (size_t)vrow[i] * P.YL);
+          w1[i] = __ldg(col + (size_t)(vrow[i] + 1) * P.YL);
+        }
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+          const float wgt = ok[i] ? rcp_approx(1.0f + ex2_approx(qv[i] + cv.C)) : 0.0f;
+          res[c * CH + i] = fmaf(wgt, blend(w0[i], w1[i], cv.fu, fz[i]), res[c * CH + i]);
+        }
+      }
     }
   }
   float* out = vol + ((size_t)yi * P.XN + xi) * P.ZN + z0;
 #pragma unroll
   for (int m = 0; m < NZ; ++m)
     if (z0 + m < P.ZN) out[m] = res[m] * P.DeltaFai;
+}
+
+// ---- packed FP32x2 arithmetic (sm_100: one instruction for two lanes) ----
+__device__ __forceinline__ uint64_t pk2(float a, float b) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void up2(uint64_t r, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// Two slices per instruction: slices (2c, 2c+1) of the thread share packed
+// registers through the row position, the bilinear blend, the weight and the
+// accumulation; the two table entries come in one 128-bit load and the
+// window test is one uniform branch per pair. Same operations per (voxel,
+// view) as bp_fast_kernel, in the same view order.
+template <int NZ>
+__global__ void __launch_bounds__(kBx* kBy) bp_fast_pair_kernel(float* __restrict__ vol,
+                                                               const uint32_t* __restrict__ fpb,
+                                                               const float2* __restrict__ trig,
+                                                               const float2* __restrict__ ztab,
+                                                               const uint32_t* __restrict__ zmask,
+                                                               const int2* __restrict__ zblock,
+                                                               const int* __restrict__ zoff, FastParams P,
+                                                               int b_first) {
+  static_assert(NZ % 2 == 0, "slices are processed in pairs");
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  const int b = b_first + blockIdx.z;
+  const int z0 = b * NZ;
+  if (xi >= P.XN || yi >= P.YN) return;
+  const int2 blk = zblock[b];
+  const int off = zoff[b];
+  const float x = ((float)xi - P.XNC) * P.dx;
+  const float y = ((float)yi - P.YNC) * P.dy;
+  uint64_t res[NZ / 2];
+#pragma unroll
+  for (int c = 0; c < NZ / 2; ++c) res[c] = 0ull;
+  const size_t plane = (size_t)P.ZL * P.YL;
+  const float4* btab = reinterpret_cast<const float4*>(ztab + (size_t)off * NZ);
+  const uint32_t* bmask = zmask + off;
+  const uint64_t half2 = pk2(-0.49999997f, -0.49999997f), magic2 = pk2(kMagic, kMagic);
+  const uint64_t one2 = pk2(1.0f, 1.0f);
+  const uint64_t zlc2 = pk2(P.ZLC0, P.ZLC0);
+  const unsigned vmax = (unsigned)(P.ZL - 2);
+  for (int q = 0; q < blk.y; ++q) {
+    const uint32_t mask = __ldg(bmask + q);
+    if (mask == 0u) continue;
+    const int p = blk.x + q;
+    ColView cv;
+    if (!col_view(P, x, y, __ldg(trig + p), cv)) continue;
+    const uint32_t* col = fpb + (size_t)p * plane + cv.u0;
+    const float4* e = btab + (size_t)q * (NZ / 2);
+    const uint64_t k2 = pk2(cv.K, cv.K), c2 = pk2(cv.C, cv.C), fu2 = pk2(cv.fu, cv.fu);
+#pragma unroll
+    for (int c = 0; c < NZ / 2; ++c) {
+      const uint32_t pm = (mask >> (2 * c)) & 3u;
+      if (pm == 0u) continue;  // uniform over the CTA
+      const float4 t = __ldg(e + c);  // {t2, Q} of slices 2c and 2c+1
+      const uint64_t v1 = fma2(pk2(t.x, t.z), k2, zlc2);
+      const uint64_t r = add2(add2(v1, half2), magic2);  // round(v1 - 1/2) in the low mantissa bits
+      const uint64_t v0f = sub2(r, magic2);
+      const uint64_t fz = sub2(v1, v0f);
+      float ra_, rb_;
+      up2(r, ra_, rb_);
+      const int va = __float_as_int(ra_) - 0x4B400000, vb = __float_as_int(rb_) - 0x4B400000;
+      const bool oka = (pm & 1u) && (unsigned)va <= vmax;
+      const bool okb = (pm & 2u) && (unsigned)vb <= vmax;
+      const uint32_t* ca = col + (size_t)(oka ? va : 0) * P.YL;
+      const uint32_t* cb = col + (size_t)(okb ? vb : 0) * P.YL;
+      const uint32_t wa0 = __ldg(ca), wa1 = __ldg(ca + P.YL);
+      const uint32_t wb0 = __ldg(cb), wb1 = __ldg(cb + P.YL);
+      // (slice a, slice b) lanes: row V0 taps u, u+1 and row V0+1 taps u, u+1
+      const uint64_t r0u0 = pk2(__uint_as_float(wa0 << 16), __uint_as_float(wb0 << 16));
+      const uint64_t r0u1 = pk2(__uint_as_float(wa0 & 0xffff0000u), __uint_as_float(wb0 & 0xffff0000u));
+      const uint64_t r1u0 = pk2(__uint_as_float(wa1 << 16), __uint_as_float(wb1 << 16));
+      const uint64_t r1u1 = pk2(__uint_as_float(wa1 & 0xffff0000u), __uint_as_float(wb1 & 0xffff0000u));
+      const uint64_t ra = fma2(fu2, sub2(r0u1, r0u0), r0u0);
+      const uint64_t rb = fma2(fu2, sub2(r1u1, r1u0), r1u0);
+      const uint64_t tap = fma2(fz, sub2(rb, ra), ra);
+      float xa, xb;
+      up2(add2(pk2(t.y, t.w), c2), xa, xb);
+      float sa, sb;
+      up2(add2(pk2(ex2_approx(xa), ex2_approx(xb)), one2), sa, sb);
+      const uint64_t wgt = pk2(oka ? rcp_approx(sa) : 0.0f, okb ? rcp_approx(sb) : 0.0f);
+      res[c] = fma2(wgt, tap, res[c]);
+    }
+  }
+  float* out = vol + ((size_t)yi * P.XN + xi) * P.ZN + z0;
+#pragma unroll
+  for (int c = 0; c < NZ / 2; ++c) {
+    float a, bb;
+    up2(res[c], a, bb);
+    if (z0 + 2 * c < P.ZN) out[2 * c] = a * P.DeltaFai;
+    if (z0 + 2 * c + 1 < P.ZN) out[2 * c + 1] = bb * P.DeltaFai;
+  }
 }
 
 // fp32 [n][YL] rows -> BF16 pairs (u, u+1), round to nearest even.
@@ -152,10 +319,9 @@ __global__ void pack_pairs_kernel(uint32_t* __restrict__ out, const float* __res
 
 namespace hr {
 
-// Host-side table build, FP64 (the reference's view angle, source height and
-// window rules, ..._3DWeighting.cpp:61-75, 79, 95-102).
-int bp_fast_create(BpFast* f, const BpFastGeom& g, const double* w) {
-  constexpr int NZ = kBpFastNz;
+// Host-side table build for NZ slices per thread, FP64 (the reference's view
+// angle, source height and window rules, ..._3DWeighting.cpp:61-75, 79, 95-102).
+static int build_tables(BpFastTables* t, int NZ, const BpFastGeom& g, const double* w) {
   const int nblocks = (g.ZN + NZ - 1) / NZ;
   std::vector<int> s0(g.ZN), lo(g.ZN), hi(g.ZN);
   std::vector<double> zc(g.ZN);
@@ -173,7 +339,7 @@ int bp_fast_create(BpFast* f, const BpFastGeom& g, const double* w) {
       hi[zi] = 0;
     }
   }
-  std::vector<int> first(nblocks), count(nblocks), off(nblocks);
+  std::vector<int> zb(3 * nblocks);
   size_t total = 0;
   for (int b = 0; b < nblocks; ++b) {
     int a = 0x7fffffff, e = -1;
@@ -188,71 +354,74 @@ int bp_fast_create(BpFast* f, const BpFastGeom& g, const double* w) {
       a = 0;
       e = -1;
     }
-    first[b] = a;
-    count[b] = e - a + 1;
-    off[b] = (int)total;
-    total += (size_t)count[b];
+    zb[2 * b] = a;                   // first view of the block's union window
+    zb[2 * b + 1] = e - a + 1;       // its number of views
+    zb[2 * nblocks + b] = (int)total;  // table row of its first view
+    total += (size_t)(e - a + 1);
   }
   HR_REQUIRE(total < (1ull << 31) / NZ, "fast backprojection: z-block table too large");
   std::vector<float2> tab(total * NZ, make_float2(0.f, 0.f));
   std::vector<uint32_t> mask(total, 0u);
   for (int b = 0; b < nblocks; ++b) {
-    for (int q = 0; q < count[b]; ++q) {
-      const int p = first[b] + q;
+    for (int q = 0; q < zb[2 * b + 1]; ++q) {
+      const int p = zb[2 * b] + q;
       const double View = g.BetaS + p * g.DeltaFai;
       const double hv = g.h * View * kInvTwoPi;
       uint32_t mk = 0;
+      const size_t row = (size_t)zb[2 * nblocks + b] + q;
       for (int m = 0; m < NZ; ++m) {
         const int zi = b * NZ + m;
         if (zi >= g.ZN || p < lo[zi] || p > hi[zi]) continue;
         const double t2 = zc[zi] - hv;
         const int d1 = (int)(g.N_pi - (double)(s0[zi] - p));
         const int d2 = p < s0[zi] ? (int)(d1 + g.N_pi) : (int)(d1 - g.N_pi);
-        const double w1 = w[d1], w2 = w[d2];
         const double tc = p < s0[zi] ? t2 - 0.5 : t2 + 0.5;
         double Q = g.k1 * (std::log2(std::fabs(t2)) - std::log2(std::fabs(tc)));
-        Q += std::log2(w2) - std::log2(w1);
-        tab[(size_t)(off[b] + q) * NZ + m] = make_float2((float)t2, (float)Q);
+        Q += std::log2(w[d2]) - std::log2(w[d1]);
+        tab[row * NZ + m] = make_float2((float)t2, (float)Q);
         mk |= 1u << m;
       }
-      mask[off[b] + q] = mk;
+      mask[row] = mk;
     }
   }
+  t->nz = NZ;
+  t->nblocks = nblocks;
+  HR_CUDA_TRY(cudaMalloc(&t->d_tab, sizeof(float2) * std::max<size_t>(tab.size(), 1)));
+  HR_CUDA_TRY(cudaMalloc(&t->d_mask, sizeof(uint32_t) * std::max<size_t>(mask.size(), 1)));
+  HR_CUDA_TRY(cudaMalloc(&t->d_zblock, sizeof(int) * zb.size()));
+  HR_CUDA_TRY(cudaMemcpy(t->d_tab, tab.data(), sizeof(float2) * tab.size(), cudaMemcpyHostToDevice));
+  HR_CUDA_TRY(cudaMemcpy(t->d_mask, mask.data(), sizeof(uint32_t) * mask.size(), cudaMemcpyHostToDevice));
+  HR_CUDA_TRY(cudaMemcpy(t->d_zblock, zb.data(), sizeof(int) * zb.size(), cudaMemcpyHostToDevice));
+  t->bytes = sizeof(float2) * tab.size() + sizeof(uint32_t) * mask.size() + sizeof(int) * zb.size();
+  return HR_OK;
+}
+
+int bp_fast_create(BpFast* f, const BpFastGeom& g, const double* w) {
+  for (int i = 0; i < kFastTableSets; ++i) HR_TRY(build_tables(&f->t[i], kFastNz[i], g, w));
   std::vector<float2> trig(g.PN);
   for (int p = 0; p < g.PN; ++p) {
     const double View = g.BetaS + p * g.DeltaFai;
     trig[p] = make_float2((float)std::cos(View), (float)std::sin(View));
   }
-  // zblock records: [nblocks] int2 {first, count}, then [nblocks] int offsets
-  std::vector<int> zb(3 * nblocks);
-  for (int b = 0; b < nblocks; ++b) {
-    zb[2 * b] = first[b];
-    zb[2 * b + 1] = count[b];
-    zb[2 * nblocks + b] = off[b];
-  }
-  f->nblocks = nblocks;
-  HR_CUDA_TRY(cudaMalloc(&f->d_tab, sizeof(float2) * tab.size()));
-  HR_CUDA_TRY(cudaMalloc(&f->d_mask, sizeof(uint32_t) * (mask.size() + 1)));
   HR_CUDA_TRY(cudaMalloc(&f->d_trig, sizeof(float2) * trig.size()));
-  HR_CUDA_TRY(cudaMalloc(&f->d_zblock, sizeof(int) * zb.size()));
-  HR_CUDA_TRY(cudaMemcpy(f->d_tab, tab.data(), sizeof(float2) * tab.size(), cudaMemcpyHostToDevice));
-  HR_CUDA_TRY(cudaMemcpy(f->d_mask, mask.data(), sizeof(uint32_t) * mask.size(), cudaMemcpyHostToDevice));
   HR_CUDA_TRY(cudaMemcpy(f->d_trig, trig.data(), sizeof(float2) * trig.size(), cudaMemcpyHostToDevice));
-  HR_CUDA_TRY(cudaMemcpy(f->d_zblock, zb.data(), sizeof(int) * zb.size(), cudaMemcpyHostToDevice));
-  f->bytes = sizeof(float2) * tab.size() + sizeof(uint32_t) * mask.size() + sizeof(float2) * trig.size() +
-             sizeof(int) * zb.size();
+  f->bytes = sizeof(float2) * trig.size();
+  for (int i = 0; i < kFastTableSets; ++i) f->bytes += f->t[i].bytes;
+  f->variant = kFastDefaultVariant;
   return HR_OK;
 }
 
 void bp_fast_destroy(BpFast* f) {
-  cudaFree(f->d_tab);
-  cudaFree(f->d_mask);
+  for (int i = 0; i < kFastTableSets; ++i) {
+    cudaFree(f->t[i].d_tab);
+    cudaFree(f->t[i].d_mask);
+    cudaFree(f->t[i].d_zblock);
+  }
   cudaFree(f->d_trig);
-  cudaFree(f->d_zblock);
   *f = BpFast{};
 }
 
-int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s) {
+static FastParams make_params(const BpFastGeom& g) {
   FastParams P;
   P.XN = g.XN; P.YN = g.YN; P.ZN = g.ZN; P.YL = g.YL; P.ZL = g.ZL; P.PN = g.PN;
   P.XNC = (float)g.XNC; P.YNC = (float)g.YNC; P.dx = (float)g.dx; P.dy = (float)g.dy;
@@ -263,11 +432,105 @@ int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint
   P.ZLC0 = (float)g.ZLC;
   P.k1 = (float)g.k1;
   P.DeltaFai = (float)g.DeltaFai;
-  dim3 grid((g.XN + kBx - 1) / kBx, (g.YN + kBy - 1) / kBy, f.nblocks);
-  HR_REQUIRE(grid.y <= 65535 && grid.z <= 65535, "fast backprojection: grid too large");
-  bp_fast_kernel<kBpFastNz><<<grid, dim3(kBx, kBy), 0, s>>>(
-      vol, fpb, f.d_trig, f.d_tab, f.d_mask, reinterpret_cast<const int2*>(f.d_zblock), f.d_zblock + 2 * f.nblocks, P);
+  return P;
+}
+
+template <int NZ, int CH>
+static void launch_variant(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol,
+                           const uint32_t* fpb, int b_first, int b_count, cudaStream_t s) {
+  dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
+  bp_fast_kernel<NZ, CH><<<grid, dim3(kBx, kBy), 0, s>>>(vol, fpb, f.d_trig, t.d_tab, t.d_mask,
+                                                          reinterpret_cast<const int2*>(t.d_zblock),
+                                                          t.d_zblock + 2 * t.nblocks, P, b_first);
+}
+
+template <int NZ>
+static void launch_pair_variant(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol,
+                                const uint32_t* fpb, int b_first, int b_count, cudaStream_t s) {
+  dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
+  bp_fast_pair_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, fpb, f.d_trig, t.d_tab, t.d_mask,
+                                                           reinterpret_cast<const int2*>(t.d_zblock),
+                                                           t.d_zblock + 2 * t.nblocks, P, b_first);
+}
+
+// Launches variant v over z blocks [b_first, b_first + b_count) (count < 0: all).
+static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, const uint32_t* fpb, int b_first,
+                       int b_count, cudaStream_t s) {
+  const FastVariant& fv = kFastVariants[v];
+  const BpFastTables& t = f.t[fv.table];
+  if (b_count < 0) b_count = t.nblocks;
+  HR_REQUIRE((g.YN + kBy - 1) / kBy <= 65535 && b_count <= 65535, "fast backprojection: grid too large");
+  if (b_count == 0) return HR_OK;
+  const FastParams P = make_params(g);
+  switch (v) {
+    case 0: launch_variant<16, 0>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 1: launch_variant<16, 4>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 2: launch_variant<16, 8>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 3: launch_variant<8, 0>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 4: launch_variant<8, 4>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 5: launch_variant<8, 8>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 6: launch_pair_variant<16>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 7: launch_pair_variant<8>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    default: return hr::fail(HR_ERR_INVALID_ARGUMENT, "fast backprojection: unknown variant %d", v);
+  }
   HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
+int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s) {
+  return run_variant(f, g, f.variant, vol, fpb, 0, -1, s);
+}
+
+// Times every variant on the same middle band of 32 slices (all columns) and
+// keeps the fastest. The band is written into vol; synchronises the stream.
+int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s) {
+  cudaEvent_t e0, e1;
+  HR_CUDA_TRY(cudaEventCreate(&e0));
+  HR_CUDA_TRY(cudaEventCreate(&e1));
+  const int band = 32;
+  const int z_first = std::max(0, g.ZN / 2 - band / 2);
+  float best = 1e30f;
+  int best_v = f->variant;
+  int st = HR_OK;
+  for (int v = 0; v < kFastVariants_n && st == HR_OK; ++v) {
+    const int nz = kFastNz[kFastVariants[v].table];
+    const int b0 = z_first / nz;
+    const int bc = std::min((band + nz - 1) / nz, f->t[kFastVariants[v].table].nblocks - b0);
+    float ms = 1e30f;
+    for (int rep = 0; rep < 3 && st == HR_OK; ++rep) {
+      cudaEventRecord(e0, s);
+      st = run_variant(*f, g, v, vol, fpb, b0, bc, s);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "fast backprojection autotune failed");
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep > 0) ms = std::min(ms, t / (float)(bc * nz));  // per slice
+    }
+    f->tuned_ms[v] = ms;
+    if (ms < best) {
+      best = ms;
+      best_v = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != HR_OK) return st;
+  f->variant = best_v;
+  f->tuned = 1;
+  return HR_OK;
+}
+
+int bp_fast_describe(const BpFast& f, char* buf, int len) {
+  if (!buf || len <= 0) return HR_OK;
+  const FastVariant& fv = kFastVariants[f.variant];
+  int n = snprintf(buf, (size_t)len, "slices_per_thread=%d gathers=%s tile=8x16 %s", kFastNz[fv.table],
+                   fv.chunk < 0 ? "paired-f32x2" : fv.chunk == 0 ? "per-slice" : fv.chunk == 4 ? "chunk4" : "chunk8",
+                   f.tuned ? "(autotuned; ms/slice:" : "(default)");
+  if (f.tuned) {
+    for (int v = 0; v < kFastVariants_n && n > 0 && n < len; ++v)
+      n += snprintf(buf + n, (size_t)(len - n), " v%d=%.4f", v, f.tuned_ms[v]);
+    if (n > 0 && n < len) snprintf(buf + n, (size_t)(len - n), ")");
+  }
   return HR_OK;
 }
 

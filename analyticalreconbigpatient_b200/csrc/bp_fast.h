@@ -3,29 +3,52 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 
 namespace hr {
-
-constexpr int kBpFastNz = 16;  // z slices per thread (one CTA covers one z block)
 
 struct BpFastGeom {
   int XN, YN, ZN, YL, ZL, PN, half;
   double XNC, YNC, ZNC, dx, dy, dz, YLC, ZLC, dYL, dZL, h, BetaS, DeltaFai, N_pi, SO, SD, k1;
 };
 
-struct BpFast {
-  int nblocks = 0;
+// Slices per thread of the two table sets (a CTA covers one z block of NZ slices).
+constexpr int kFastTableSets = 2;
+constexpr int kFastNz[kFastTableSets] = {16, 8};
+
+// Kernel variants the autotuner chooses from: table set and gather chunk
+// (0 = one slice at a time, 4/8 = slices whose gathers are issued together,
+// -1 = slice pairs in packed FP32x2 arithmetic).
+struct FastVariant {
+  int table, chunk;
+};
+constexpr FastVariant kFastVariants[] = {{0, 0}, {0, 4}, {0, 8}, {1, 0}, {1, 4}, {1, 8}, {0, -1}, {1, -1}};
+constexpr int kFastVariants_n = sizeof(kFastVariants) / sizeof(kFastVariants[0]);
+constexpr int kFastDefaultVariant = 0;
+
+struct BpFastTables {
+  int nz = 0, nblocks = 0;
   float2* d_tab = nullptr;     // per z block and view of its window: NZ x {t2, Q}
   uint32_t* d_mask = nullptr;  // per z block and view: slices whose [s1, s2] holds the view
-  float2* d_trig = nullptr;    // per view: {cos, sin}
   int* d_zblock = nullptr;     // [nblocks] {first view, count}, then [nblocks] table offsets
+  size_t bytes = 0;
+};
+
+struct BpFast {
+  BpFastTables t[kFastTableSets];
+  float2* d_trig = nullptr;  // per view: {cos, sin}
+  int variant = kFastDefaultVariant;
+  int tuned = 0;
+  float tuned_ms[kFastVariants_n] = {};  // autotuner: ms per slice of each variant
   size_t bytes = 0;
 };
 
 int bp_fast_create(BpFast* f, const BpFastGeom& g, const double* w);
 void bp_fast_destroy(BpFast* f);
 int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s);
+int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s);
+int bp_fast_describe(const BpFast& f, char* buf, int len);
 // FP32 rows [rows][YL] -> BF16 channel pairs: word u = bf16(x[u]) | bf16(x[u+1]) << 16.
 int pack_pairs(uint32_t* out, const float* in, long long rows, int YL, cudaStream_t s);
 

@@ -86,11 +86,27 @@ extern "C" int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* d
     cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "hr_recon_plan_create: %s", cudaGetErrorString(e));
   }
+  if (st == HR_OK && fast) {
+    // pick the backprojection variant on the plan's own (zeroed) buffers
+    cudaError_t e = cudaMemsetAsync(p->d_pairs, 0, nfilt * sizeof(uint32_t), p->stream);
+    if (e != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "hr_recon_plan_create: %s", cudaGetErrorString(e));
+    if (st == HR_OK) st = hr_bp_autotune(p->bp, p->d_vol, p->d_pairs, p->stream);
+  }
   if (st != HR_OK) {
     destroy(p);
     return st;
   }
   *plan = p;
+  return HR_OK;
+}
+
+extern "C" int hr_recon_describe(const hr_recon_plan* p, char* buf, int len) {
+  HR_REQUIRE(p != nullptr, "hr_recon_describe: NULL plan");
+  char bp[256];
+  HR_TRY(hr_bp_describe(p->bp, bp, sizeof(bp)));
+  if (buf && len > 0)
+    snprintf(buf, (size_t)len, "filter=%s; backprojection: %s",
+             p->filter_tc ? "tcgen05 split-BF16 Toeplitz" : "FP32 radix-4 FFT", bp);
   return HR_OK;
 }
 

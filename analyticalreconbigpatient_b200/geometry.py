@@ -248,6 +248,8 @@ def config(name: str) -> Scan:
     if name == "full":
         return Scan(ZL=64, pitch=0.984, rotations=20, XN=512, YN=512, ZN=1, dx=0.9766, dy=0.9766,
                     dz=0.625).with_full_z()
+    if name == "medium":  # full detector and grid spacing, 2 rotations: a profiling-size case
+        return Scan(ZL=64, pitch=0.984, rotations=2, XN=512, YN=512, ZN=48, dx=0.9766, dy=0.9766, dz=0.625)
     if name == "halfview":
         return Scan(ZL=64, pitch=0.984, rotations=10, N_2pi=492, XN=512, YN=512, ZN=1, dx=0.9766, dy=0.9766,
                     dz=0.625).with_full_z()

@@ -68,6 +68,11 @@ class HelicalRecon:
         """Raise if a kernel of an earlier execution reported a timed-out pipeline wait (synchronises)."""
         _lib.check(_lib.load().hr_recon_check(self._plan))
 
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        _lib.check(_lib.load().hr_recon_describe(self._plan, buf, 512))
+        return buf.value.decode()
+
     def run(self, fan: torch.Tensor, volume: torch.Tensor | None = None, stream=None) -> torch.Tensor:
         """fan: device float32 [views][YL][ZL] (post-flip channel order)."""
         vol = self.volume if volume is None else volume
@@ -139,6 +144,13 @@ class StagePlans:
     def check(self) -> None:
         if self._filter_tc:
             _lib.check(_lib.load().hr_filter_tc_check(self._filter_tc))
+
+    def autotune(self, vol: torch.Tensor, fp: torch.Tensor, stream: int = 0) -> str:
+        lib = _lib.load()
+        _lib.check(lib.hr_bp_autotune(self._bp, vol.data_ptr(), fp.data_ptr(), stream))
+        buf = ctypes.create_string_buffer(256)
+        _lib.check(lib.hr_bp_describe(self._bp, buf, 256))
+        return buf.value.decode()
 
     def pack(self, out: torch.Tensor, filtered: torch.Tensor, stream: int = 0) -> None:
         """FP32 filtered rows -> BF16 channel pairs (the fast form's layout)."""

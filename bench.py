@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["full", "small"], default="full")
+    ap.add_argument("--config", choices=["full", "medium", "small"], default="full")
     ap.add_argument("--form", choices=["fast", "plain"], default="fast",
                     help="form timed as `value` (the chosen BF16 form by default); the plain FP32 form is "
                          "timed beside it unless --no-plain")
@@ -251,6 +251,10 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
     filtered = None if fast else torch.empty((scan.PN, scan.ZL, scan.YL), dtype=torch.float32, device=dev)
     pairs = torch.empty((scan.PN, scan.ZL, scan.YL), dtype=torch.int32, device=dev) if fast else None
     vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, device=dev)
+    if fast:  # the chain plan autotunes its backprojection at creation; do the same for the stage plans
+        stages.rebin(rebinned, fan, st)
+        stages.filter_tc(pairs, rebinned, _lib.HR_LAYOUT_REBIN, scan.crop_front, st)
+        stages.autotune(vol, pairs, st)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     names = ["rebin", "filter", "backprojection"]
     stage_ms = {k: [] for k in names}
@@ -296,7 +300,7 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
         ms = float(tm.item())
     rec.check()
     out = {"ms_per_step": ms, "stages_ms": {k: statistics.mean(v) for k, v in stage_ms.items() if v},
-           "launches_per_step": 4 if fast else 3}
+           "launches_per_step": 4 if fast else 3, "kernels": rec.describe()}
 
     # ---- end to end through the C ABI host entry -----------------------------
     if with_e2e:
@@ -351,7 +355,7 @@ def main():
     # ---- data (each rank its own seeded phantom) ------------------------------
     zlo = scan.h * scan.BetaS / (2 * np.pi)
     zhi = scan.h * (scan.BetaS + scan.views * scan.dBeta) / (2 * np.pi)
-    objs = P.random_ellipsoids(1000 + rank, 60, (zlo, zhi)) if args.config == "full" else P.shepp_logan()
+    objs = P.random_ellipsoids(1000 + rank, 60, (zlo, zhi)) if args.config != "small" else P.shepp_logan()
     fan = project(scan, objs, device=local)
     updates = scan.updates()
     chosen = _lib.HR_FORM_FAST if args.form == "fast" else _lib.HR_FORM_PLAIN
@@ -403,6 +407,7 @@ def main():
                     "h2d_bytes_per_step": scan.projection_bytes(), "d2h_bytes_per_step": scan.volume_bytes(),
                     "entry": "hr_recon_execute_host (C ABI, pinned host buffers)"},
             "gpu_launches": res["launches_per_step"] * args.steps,
+            "kernels": res["kernels"],
             "clocks": clocks.summary()}
     if plain is not None:
         pv = updates * world / (plain["ms_per_step"] * 1e-3) / 1e9

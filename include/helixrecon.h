@@ -183,6 +183,18 @@ int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const double* w, i
  * for HR_FORM_FAST); d_vol: device [YN][XN][ZN] (double for HR_FORM_FP64, else float). */
 int hr_bp_execute(const hr_bp_plan* plan, void* d_vol, const void* d_fp, void* stream);
 void hr_bp_plan_destroy(hr_bp_plan* plan);
+/* HR_FORM_FAST: times the kernel variants (slices per thread x gathers issued
+ * together) on a 32-slice band of d_vol and keeps the fastest for the plan's
+ * later executions. Synchronises the stream; call before graph capture. Other
+ * forms: no-op. */
+int hr_bp_autotune(hr_bp_plan* plan, void* d_vol, const void* d_fp, void* stream);
+/* Writes a one-line description of the kernel configuration into buf. */
+int hr_bp_describe(const hr_bp_plan* plan, char* buf, int len);
+/* Selects a fast-form kernel variant by index (the autotuner's candidates:
+ * 0-2 sixteen slices per thread, 3-5 eight, gathers issued one, four or eight
+ * slices at a time; 6-7 sixteen / eight slices per thread in packed FP32x2
+ * slice pairs). For tests and manual tuning. */
+int hr_bp_select(hr_bp_plan* plan, int variant);
 
 /* ---- backprojection that allocates nothing ------------------------------ */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc:
@@ -228,6 +240,9 @@ int hr_recon_execute(const hr_recon_plan* plan, float* d_vol, const float* d_fan
 /* Host pointers (pinned for full copy speed): copies the fan data in, runs the
  * chain, copies the volume out; returns when h_vol is written. */
 int hr_recon_execute_host(hr_recon_plan* plan, float* h_vol, const float* h_fan);
+/* One-line description of the plan's kernel configuration (the fast form's
+ * backprojection is autotuned at plan creation). */
+int hr_recon_describe(const hr_recon_plan* plan, char* buf, int len);
 /* Synchronous health check of the plan's kernels (tensor-core filter flag). */
 int hr_recon_check(const hr_recon_plan* plan);
 /* Device bytes the plan holds (tables + intermediate + host-staging buffers). */

@@ -106,3 +106,33 @@ def test_pack_pairs_layout(cuda):
     np.testing.assert_array_equal(lo.view(np.float32), xb)
     np.testing.assert_array_equal(hi[:, :-1].view(np.float32), xb[:, 1:])
     assert np.all(hi[:, -1] == 0)
+
+
+def test_every_fast_variant_gives_the_same_volume(cuda):
+    """The autotuner's candidates differ only in work distribution: the same
+    FP32 operations per (voxel, view) in the same view order, so identical bits."""
+    from analyticalreconbigpatient_b200.pipeline import StagePlans
+
+    sc = G.Scan(ZL=16, pitch=0.9375, rotations=3, XN=40, YN=48, ZN=37, dx=5.0, dy=5.0, dz=1.0)
+    rng = np.random.default_rng(3)
+    filt = torch.tensor(rng.standard_normal((sc.PN, sc.ZL, sc.YL)).astype(np.float32), device=cuda)
+    fast = StagePlans(sc, _lib.HR_FORM_FAST)
+    pairs = torch.empty((sc.PN, sc.ZL, sc.YL), dtype=torch.int32, device=cuda)
+    fast.pack(pairs, filt)
+    lib = _lib.load()
+    vols = []
+    nvar = 8
+    for v in range(nvar):
+        _lib.check(lib.hr_bp_select(fast._bp, v))
+        vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
+        fast.backproject(vol, pairs)
+        torch.cuda.synchronize()
+        vols.append(vol.cpu().numpy())
+    desc = fast.autotune(torch.empty_like(vol), pairs)
+    assert "autotuned" in desc
+    fast.close()
+    for v in range(1, 6):
+        assert np.array_equal(vols[v], vols[0]), v
+    for v in range(6, nvar):  # packed FP32x2 rounds like FP32, but FMA contraction may differ
+        assert rel_l2(vols[v], vols[0]) < 1e-6, v
+    assert np.isfinite(vols[0]).all()
