@@ -80,6 +80,11 @@ _SIGS = {
     "hr_filter_tc_device_bytes": (ctypes.c_size_t, [_p]),
     "hr_filter_tc_plan_destroy": (None, [_p]),
     "hr_recon_check": (_i, [_p]),
+    "hr_slab_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc), _i]),
+    "hr_slab_execute": (_i, [_p, _p, _p, _i, _i]),
+    "hr_slab_describe": (_i, [_p, ctypes.c_char_p, _i]),
+    "hr_slab_device_bytes": (ctypes.c_size_t, [_p]),
+    "hr_slab_plan_destroy": (None, [_p]),
     "hr_recon_describe": (_i, [_p, ctypes.c_char_p, _i]),
     "hr_bp_autotune": (_i, [_p, _p, _p, _p]),
     "hr_bp_describe": (_i, [_p, ctypes.c_char_p, _i]),

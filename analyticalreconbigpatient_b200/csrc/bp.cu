@@ -307,6 +307,7 @@ extern "C" int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const d
     f.XNC = g->XNC; f.YNC = g->YNC; f.ZNC = g->ZNC; f.dx = g->dx; f.dy = g->dy; f.dz = g->dz;
     f.YLC = g->YLC; f.ZLC = g->ZLC; f.dYL = g->dYL; f.dZL = g->dZL; f.h = g->h; f.BetaS = g->BetaS;
     f.DeltaFai = g->DeltaFai; f.N_pi = g->N_pi; f.SO = g->SO; f.SD = g->SD; f.k1 = g->k1;
+    f.ZN_valid = g->ZN;
     const int st = hr::bp_fast_create(&pl->fast, f, w);
     if (st != HR_OK) {
       hr::bp_fast_destroy(&pl->fast);

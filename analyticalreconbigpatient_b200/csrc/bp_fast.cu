@@ -321,7 +321,7 @@ namespace hr {
 
 // Host-side table build for NZ slices per thread, FP64 (the reference's view
 // angle, source height and window rules, ..._3DWeighting.cpp:61-75, 79, 95-102).
-static int build_tables(BpFastTables* t, int NZ, const BpFastGeom& g, const double* w) {
+static int build_host(BpFastHostSet* t, int NZ, const BpFastGeom& g, const double* w) {
   const int nblocks = (g.ZN + NZ - 1) / NZ;
   std::vector<int> s0(g.ZN), lo(g.ZN), hi(g.ZN);
   std::vector<double> zc(g.ZN);
@@ -331,7 +331,7 @@ static int build_tables(BpFastTables* t, int NZ, const BpFastGeom& g, const doub
     const double beta0 = kTwoPiTrunc * z / g.h;
     s0[zi] = (int)std::ceil((beta0 - g.BetaS) / g.DeltaFai - 0.5);
     const int s1 = s0[zi] - g.half, s2 = s0[zi] + g.half;
-    if (s1 < g.PN && s2 > 0) {
+    if (zi < g.ZN_valid && s1 < g.PN && s2 > 0) {
       lo[zi] = s1 < 0 ? 0 : s1;
       hi[zi] = s2 > g.PN - 1 ? g.PN - 1 : s2;
     } else {
@@ -339,7 +339,9 @@ static int build_tables(BpFastTables* t, int NZ, const BpFastGeom& g, const doub
       hi[zi] = 0;
     }
   }
-  std::vector<int> zb(3 * nblocks);
+  t->nz = NZ;
+  t->nblocks = nblocks;
+  t->zb.assign(3 * nblocks, 0);
   size_t total = 0;
   for (int b = 0; b < nblocks; ++b) {
     int a = 0x7fffffff, e = -1;
@@ -354,21 +356,21 @@ static int build_tables(BpFastTables* t, int NZ, const BpFastGeom& g, const doub
       a = 0;
       e = -1;
     }
-    zb[2 * b] = a;                   // first view of the block's union window
-    zb[2 * b + 1] = e - a + 1;       // its number of views
-    zb[2 * nblocks + b] = (int)total;  // table row of its first view
+    t->zb[2 * b] = a;                    // first view of the block's union window
+    t->zb[2 * b + 1] = e - a + 1;        // its number of views
+    t->zb[2 * nblocks + b] = (int)total;  // table row of its first view
     total += (size_t)(e - a + 1);
   }
   HR_REQUIRE(total < (1ull << 31) / NZ, "fast backprojection: z-block table too large");
-  std::vector<float2> tab(total * NZ, make_float2(0.f, 0.f));
-  std::vector<uint32_t> mask(total, 0u);
+  t->tab.assign(total * NZ, make_float2(0.f, 0.f));
+  t->mask.assign(total, 0u);
   for (int b = 0; b < nblocks; ++b) {
-    for (int q = 0; q < zb[2 * b + 1]; ++q) {
-      const int p = zb[2 * b] + q;
+    for (int q = 0; q < t->zb[2 * b + 1]; ++q) {
+      const int p = t->zb[2 * b] + q;
       const double View = g.BetaS + p * g.DeltaFai;
       const double hv = g.h * View * kInvTwoPi;
       uint32_t mk = 0;
-      const size_t row = (size_t)zb[2 * nblocks + b] + q;
+      const size_t row = (size_t)t->zb[2 * nblocks + b] + q;
       for (int m = 0; m < NZ; ++m) {
         const int zi = b * NZ + m;
         if (zi >= g.ZN || p < lo[zi] || p > hi[zi]) continue;
@@ -378,35 +380,72 @@ static int build_tables(BpFastTables* t, int NZ, const BpFastGeom& g, const doub
         const double tc = p < s0[zi] ? t2 - 0.5 : t2 + 0.5;
         double Q = g.k1 * (std::log2(std::fabs(t2)) - std::log2(std::fabs(tc)));
         Q += std::log2(w[d2]) - std::log2(w[d1]);
-        tab[row * NZ + m] = make_float2((float)t2, (float)Q);
+        t->tab[row * NZ + m] = make_float2((float)t2, (float)Q);
         mk |= 1u << m;
       }
-      mask[row] = mk;
+      t->mask[row] = mk;
     }
   }
-  t->nz = NZ;
-  t->nblocks = nblocks;
-  HR_CUDA_TRY(cudaMalloc(&t->d_tab, sizeof(float2) * std::max<size_t>(tab.size(), 1)));
-  HR_CUDA_TRY(cudaMalloc(&t->d_mask, sizeof(uint32_t) * std::max<size_t>(mask.size(), 1)));
-  HR_CUDA_TRY(cudaMalloc(&t->d_zblock, sizeof(int) * zb.size()));
-  HR_CUDA_TRY(cudaMemcpy(t->d_tab, tab.data(), sizeof(float2) * tab.size(), cudaMemcpyHostToDevice));
-  HR_CUDA_TRY(cudaMemcpy(t->d_mask, mask.data(), sizeof(uint32_t) * mask.size(), cudaMemcpyHostToDevice));
-  HR_CUDA_TRY(cudaMemcpy(t->d_zblock, zb.data(), sizeof(int) * zb.size(), cudaMemcpyHostToDevice));
-  t->bytes = sizeof(float2) * tab.size() + sizeof(uint32_t) * mask.size() + sizeof(int) * zb.size();
+  return HR_OK;
+}
+
+int bp_fast_host_tables(BpFastHost* h, const BpFastGeom& g, const double* w) {
+  for (int i = 0; i < kFastTableSets; ++i) HR_TRY(build_host(&h->set[i], kFastNz[i], g, w));
+  h->trig.resize(g.PN);
+  for (int p = 0; p < g.PN; ++p) {
+    const double View = g.BetaS + p * g.DeltaFai;
+    h->trig[p] = make_float2((float)std::cos(View), (float)std::sin(View));
+  }
+  return HR_OK;
+}
+
+int bp_fast_reserve(BpFast* f, const size_t rows[kFastTableSets], const int nblocks[kFastTableSets], int PN) {
+  f->bytes = 0;
+  for (int i = 0; i < kFastTableSets; ++i) {
+    BpFastTables& t = f->t[i];
+    t.nz = kFastNz[i];
+    t.nblocks = nblocks[i];
+    t.cap_rows = std::max<size_t>(rows[i], 1);
+    HR_CUDA_TRY(cudaMalloc(&t.d_tab, sizeof(float2) * t.cap_rows * t.nz));
+    HR_CUDA_TRY(cudaMalloc(&t.d_mask, sizeof(uint32_t) * t.cap_rows));
+    HR_CUDA_TRY(cudaMalloc(&t.d_zblock, sizeof(int) * 3 * (size_t)t.nblocks));
+    t.bytes = (sizeof(float2) * t.nz + sizeof(uint32_t)) * t.cap_rows + sizeof(int) * 3 * (size_t)t.nblocks;
+    f->bytes += t.bytes;
+  }
+  f->cap_views = PN;
+  HR_CUDA_TRY(cudaMalloc(&f->d_trig, sizeof(float2) * (size_t)PN));
+  f->bytes += sizeof(float2) * (size_t)PN;
+  return HR_OK;
+}
+
+int bp_fast_upload(BpFast* f, const BpFastHost& h, cudaStream_t s) {
+  for (int i = 0; i < kFastTableSets; ++i) {
+    BpFastTables& t = f->t[i];
+    const BpFastHostSet& ht = h.set[i];
+    HR_REQUIRE(ht.nblocks == t.nblocks && ht.mask.size() <= t.cap_rows,
+               "fast backprojection: tables exceed the reserved capacity");
+    HR_CUDA_TRY(cudaMemcpyAsync(t.d_tab, ht.tab.data(), sizeof(float2) * ht.tab.size(), cudaMemcpyHostToDevice, s));
+    HR_CUDA_TRY(cudaMemcpyAsync(t.d_mask, ht.mask.data(), sizeof(uint32_t) * ht.mask.size(), cudaMemcpyHostToDevice,
+                                s));
+    HR_CUDA_TRY(cudaMemcpyAsync(t.d_zblock, ht.zb.data(), sizeof(int) * ht.zb.size(), cudaMemcpyHostToDevice, s));
+  }
+  HR_REQUIRE(h.trig.size() <= (size_t)f->cap_views, "fast backprojection: more views than reserved");
+  HR_CUDA_TRY(cudaMemcpyAsync(f->d_trig, h.trig.data(), sizeof(float2) * h.trig.size(), cudaMemcpyHostToDevice, s));
   return HR_OK;
 }
 
 int bp_fast_create(BpFast* f, const BpFastGeom& g, const double* w) {
-  for (int i = 0; i < kFastTableSets; ++i) HR_TRY(build_tables(&f->t[i], kFastNz[i], g, w));
-  std::vector<float2> trig(g.PN);
-  for (int p = 0; p < g.PN; ++p) {
-    const double View = g.BetaS + p * g.DeltaFai;
-    trig[p] = make_float2((float)std::cos(View), (float)std::sin(View));
+  BpFastHost h;
+  HR_TRY(bp_fast_host_tables(&h, g, w));
+  size_t rows[kFastTableSets];
+  int nb[kFastTableSets];
+  for (int i = 0; i < kFastTableSets; ++i) {
+    rows[i] = h.set[i].mask.size();
+    nb[i] = h.set[i].nblocks;
   }
-  HR_CUDA_TRY(cudaMalloc(&f->d_trig, sizeof(float2) * trig.size()));
-  HR_CUDA_TRY(cudaMemcpy(f->d_trig, trig.data(), sizeof(float2) * trig.size(), cudaMemcpyHostToDevice));
-  f->bytes = sizeof(float2) * trig.size();
-  for (int i = 0; i < kFastTableSets; ++i) f->bytes += f->t[i].bytes;
+  HR_TRY(bp_fast_reserve(f, rows, nb, g.PN));
+  HR_TRY(bp_fast_upload(f, h, nullptr));
+  HR_CUDA_TRY(cudaStreamSynchronize(nullptr));
   f->variant = kFastDefaultVariant;
   return HR_OK;
 }

@@ -242,6 +242,9 @@ def config(name: str) -> Scan:
     full     888x64, pitch 0.984, 20 rotations, 512x512xN at 0.9766 x 0.625 mm,
              N spanning the fully sampled z range (random ellipsoid phantom)
     halfview full geometry at 492 views/rot and 10 rotations
+    bigpatient full detector, 200 rotations (196,800 views, 44.7 GB), 512x512x2000
+             with the slice thickness chosen so the 2000 slices span the fully
+             sampled z range (3.92 mm)
     """
     if name == "small":
         return Scan(ZL=16, pitch=0.9375, rotations=4, XN=256, YN=256, ZN=32, dx=1.5625, dy=1.5625, dz=1.0)
@@ -250,6 +253,10 @@ def config(name: str) -> Scan:
                     dz=0.625).with_full_z()
     if name == "medium":  # full detector and grid spacing, 2 rotations: a profiling-size case
         return Scan(ZL=64, pitch=0.984, rotations=2, XN=512, YN=512, ZN=48, dx=0.9766, dy=0.9766, dz=0.625)
+    if name == "bigpatient":  # 200 rotations; 2000 slices spanning the fully sampled z range
+        sc = Scan(ZL=64, pitch=0.984, rotations=200, XN=512, YN=512, ZN=2000, dx=0.9766, dy=0.9766, dz=1.0)
+        half = math.ceil(sc.N_2pi / 2.0 * sc.HSCoef)
+        return replace(sc, dz=sc.h * (sc.PN - 2 * half) / sc.N_2pi / sc.ZN)
     if name == "halfview":
         return Scan(ZL=64, pitch=0.984, rotations=10, N_2pi=492, XN=512, YN=512, ZN=1, dx=0.9766, dy=0.9766,
                     dz=0.625).with_full_z()

@@ -105,6 +105,50 @@ class HelicalRecon:
             pass
 
 
+class SlabRecon:
+    """Long scans reconstructed slab by slab (disjoint z slabs, each from its own
+    view window) through a captured CUDA graph; see hr_slab_plan in
+    include/helixrecon.h. Fast form only."""
+
+    def __init__(self, scan: Scan, slab_slices: int = 64, device: int | torch.device = 0):
+        self.scan = scan
+        self.device = torch.device("cuda", device) if isinstance(device, int) else device
+        self._plan = ctypes.c_void_p()
+        w = view_weights(scan)
+        desc = recon_desc(scan, w, _lib.HR_FORM_FAST)
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().hr_slab_plan_create(ctypes.byref(self._plan), ctypes.byref(desc), slab_slices))
+
+    def run(self, fan, volume) -> None:
+        """fan/volume: torch tensors (CUDA or CPU; pinned CPU tensors overlap copies with compute)."""
+        def ptr(t):
+            return (t.data_ptr(), 0) if t.is_cuda else (t.data_ptr(), 1)
+        fp, fh = ptr(fan)
+        vp, vh = ptr(volume)
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().hr_slab_execute(self._plan, vp, fp, vh, fh))
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(768)
+        _lib.check(_lib.load().hr_slab_describe(self._plan, buf, 768))
+        return buf.value.decode()
+
+    @property
+    def device_bytes(self) -> int:
+        return int(_lib.load().hr_slab_device_bytes(self._plan))
+
+    def close(self) -> None:
+        if self._plan:
+            _lib.load().hr_slab_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class StagePlans:
     """The three stage plans of a scan, for per-stage use and the FP64 form."""
 

@@ -249,6 +249,24 @@ int hr_recon_check(const hr_recon_plan* plan);
 size_t hr_recon_device_bytes(const hr_recon_plan* plan);
 void hr_recon_plan_destroy(hr_recon_plan* plan);
 
+/* ---- slab-batched long scans (big patients) ------------------------------ */
+/* Replaces the segment loop of src/analyticalRecon.m:15-25 (segments of views,
+ * each reconstructed into the whole volume and summed) by disjoint z slabs:
+ * each slab of slab_slices slices is reconstructed from only its own view
+ * window (plus the half-fan margin) through one captured CUDA graph (rebin ->
+ * tensor-core filter -> fast backprojection, autotuned on the first call);
+ * fan windows stream in on a second stream while the previous slab computes.
+ * desc: the whole scan (form HR_FORM_FAST; the crop view0 must be the same at
+ * both ends, as the geometry helpers make it). */
+typedef struct hr_slab_plan hr_slab_plan;
+int hr_slab_plan_create(hr_slab_plan** plan, const hr_recon_desc* desc, int slab_slices);
+/* fan [ViewN][YL][ZL], vol [YN][XN][ZN]; each on the host (pinned for overlap)
+ * or the device as the flags say. Synchronous. */
+int hr_slab_execute(hr_slab_plan* plan, float* vol, const float* fan, int vol_on_host, int fan_on_host);
+int hr_slab_describe(const hr_slab_plan* plan, char* buf, int len);
+size_t hr_slab_device_bytes(const hr_slab_plan* plan);
+void hr_slab_plan_destroy(hr_slab_plan* plan);
+
 /* ---- analytic phantom projector (synthetic data source) ----------------- */
 /* Objects: nobj rows of 17 doubles [type, cx, cy, cz, a, b, c, R(9, row-major,
  * columns = body axes), mu]; type 0 ellipsoid, type 1 elliptic cylinder (z in
