@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "hr_internal.h"
@@ -510,6 +511,9 @@ static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, 
     case 5: launch_variant<8, 8>(t, f, P, vol, fpb, b_first, b_count, s); break;
     case 6: launch_pair_variant<16>(t, f, P, vol, fpb, b_first, b_count, s); break;
     case 7: launch_pair_variant<8>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 8: launch_variant<4, 0>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 9: launch_pair_variant<4>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 10: launch_variant<4, 4>(t, f, P, vol, fpb, b_first, b_count, s); break;
     default: return hr::fail(HR_ERR_INVALID_ARGUMENT, "fast backprojection: unknown variant %d", v);
   }
   HR_CUDA_TRY(cudaGetLastError());
@@ -522,7 +526,26 @@ int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint
 
 // Times every variant on the same middle band of 32 slices (all columns) and
 // keeps the fastest. The band is written into vol; synchronises the stream.
+// HELIXRECON_BP_VARIANT=<index> pins the variant and skips the timing (for
+// profiling runs, whose serialised launches would skew the choice, and for
+// reproducible benchmarks).
+static int pinned_variant() {
+  const char* e = std::getenv("HELIXRECON_BP_VARIANT");
+  if (!e || !*e) return -1;
+  char* end = nullptr;
+  const long v = std::strtol(e, &end, 10);
+  if (*end != '\0' || v < 0 || v >= kFastVariants_n) return -2;
+  return (int)v;
+}
+
 int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s) {
+  const int pin = pinned_variant();
+  HR_REQUIRE(pin != -2, "HELIXRECON_BP_VARIANT must be an integer in [0, %d)", kFastVariants_n);
+  if (pin >= 0) {
+    f->variant = pin;
+    f->tuned = 2;
+    return HR_OK;
+  }
   cudaEvent_t e0, e1;
   HR_CUDA_TRY(cudaEventCreate(&e0));
   HR_CUDA_TRY(cudaEventCreate(&e1));
@@ -564,8 +587,9 @@ int bp_fast_describe(const BpFast& f, char* buf, int len) {
   const FastVariant& fv = kFastVariants[f.variant];
   int n = snprintf(buf, (size_t)len, "slices_per_thread=%d gathers=%s tile=8x16 %s", kFastNz[fv.table],
                    fv.chunk < 0 ? "paired-f32x2" : fv.chunk == 0 ? "per-slice" : fv.chunk == 4 ? "chunk4" : "chunk8",
-                   f.tuned ? "(autotuned; ms/slice:" : "(default)");
-  if (f.tuned) {
+                   f.tuned == 2 ? "(pinned by HELIXRECON_BP_VARIANT)"
+                   : f.tuned ? "(autotuned; ms/slice:" : "(default)");
+  if (f.tuned == 1) {
     for (int v = 0; v < kFastVariants_n && n > 0 && n < len; ++v)
       n += snprintf(buf + n, (size_t)(len - n), " v%d=%.4f", v, f.tuned_ms[v]);
     if (n > 0 && n < len) snprintf(buf + n, (size_t)(len - n), ")");

@@ -15,9 +15,11 @@ struct BpFastGeom {
   double XNC, YNC, ZNC, dx, dy, dz, YLC, ZLC, dYL, dZL, h, BetaS, DeltaFai, N_pi, SO, SD, k1;
 };
 
-// Slices per thread of the two table sets (a CTA covers one z block of NZ slices).
-constexpr int kFastTableSets = 2;
-constexpr int kFastNz[kFastTableSets] = {16, 8};
+// Slices per thread of the table sets (a CTA covers one z block of NZ slices);
+// thin slices favour 8-16 (per-view work shared by more slices), thick slices
+// 4 (adjacent slices' view windows overlap less).
+constexpr int kFastTableSets = 3;
+constexpr int kFastNz[kFastTableSets] = {16, 8, 4};
 
 // Kernel variants the autotuner chooses from: table set and gather chunk
 // (0 = one slice at a time, 4/8 = slices whose gathers are issued together,
@@ -25,7 +27,8 @@ constexpr int kFastNz[kFastTableSets] = {16, 8};
 struct FastVariant {
   int table, chunk;
 };
-constexpr FastVariant kFastVariants[] = {{0, 0}, {0, 4}, {0, 8}, {1, 0}, {1, 4}, {1, 8}, {0, -1}, {1, -1}};
+constexpr FastVariant kFastVariants[] = {{0, 0}, {0, 4}, {0, 8}, {1, 0}, {1, 4}, {1, 8},
+                                         {0, -1}, {1, -1}, {2, 0}, {2, -1}, {2, 4}};
 constexpr int kFastVariants_n = sizeof(kFastVariants) / sizeof(kFastVariants[0]);
 constexpr int kFastDefaultVariant = 0;
 

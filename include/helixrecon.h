@@ -193,7 +193,8 @@ int hr_bp_describe(const hr_bp_plan* plan, char* buf, int len);
 /* Selects a fast-form kernel variant by index (the autotuner's candidates:
  * 0-2 sixteen slices per thread, 3-5 eight, gathers issued one, four or eight
  * slices at a time; 6-7 sixteen / eight slices per thread in packed FP32x2
- * slice pairs). For tests and manual tuning. */
+ * slice pairs; 8-10 four slices per thread, per slice / pairs / batched).
+ * For tests and manual tuning. */
 int hr_bp_select(hr_bp_plan* plan, int variant);
 
 /* ---- backprojection that allocates nothing ------------------------------ */

@@ -90,3 +90,10 @@ def test_configs_build(name):
     sc = G.config(name)
     assert sc.PN > 2 * math.ceil(sc.N_2pi / 2 * sc.HSCoef)
     assert sc.updates() > 0
+
+
+def test_bigpatient_geometry_spans_the_scan():
+    sc = G.config("bigpatient")
+    assert sc.views == 196800 and sc.ZN == 2000
+    assert abs(sc.ZN * sc.dz - sc.h * (sc.PN - 2 * 335) / 984) < 1e-6 * sc.ZN * sc.dz
+    assert np.all(sc.window_per_slice() == 671)

@@ -121,7 +121,7 @@ def test_every_fast_variant_gives_the_same_volume(cuda):
     fast.pack(pairs, filt)
     lib = _lib.load()
     vols = []
-    nvar = 8
+    nvar = 11
     for v in range(nvar):
         _lib.check(lib.hr_bp_select(fast._bp, v))
         vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
@@ -131,8 +131,8 @@ def test_every_fast_variant_gives_the_same_volume(cuda):
     desc = fast.autotune(torch.empty_like(vol), pairs)
     assert "autotuned" in desc
     fast.close()
-    for v in range(1, 6):
+    for v in (1, 2, 3, 4, 5, 8, 10):
         assert np.array_equal(vols[v], vols[0]), v
-    for v in range(6, nvar):  # packed FP32x2 rounds like FP32, but FMA contraction may differ
+    for v in (6, 7, 9):  # packed FP32x2 rounds like FP32, but FMA contraction may differ
         assert rel_l2(vols[v], vols[0]) < 1e-6, v
     assert np.isfinite(vols[0]).all()

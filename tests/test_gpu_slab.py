@@ -47,9 +47,3 @@ def test_slabs_match_whole_scan_fast_chain(cuda, slab, dz):
     assert np.array_equal(vol_h.numpy(), got)
     rec.close()
 
-
-def test_bigpatient_geometry_spans_the_scan(cuda):
-    sc = G.config("bigpatient")
-    assert sc.views == 196800 and sc.ZN == 2000
-    assert abs(sc.ZN * sc.dz - sc.h * (sc.PN - 2 * 335) / 984) < 1e-6 * sc.ZN * sc.dz
-    assert np.all(sc.window_per_slice() == 671)
