@@ -90,6 +90,25 @@ _SIGS = {
     "hr_bp_describe": (_i, [_p, ctypes.c_char_p, _i]),
     "hr_bp_select": (_i, [_p, _i]),
     "hr_bp_plain_noalloc": (_i, [_p, _p, _p, ctypes.POINTER(BpGeom), _p]),
+    "hr_batch_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc), _i]),
+    "hr_batch_execute": (_i, [_p, _p, _p, _p]),
+    "hr_batch_select": (_i, [_p, _i]),
+    "hr_batch_backproject": (_i, [_p, _p, _p]),
+    "hr_batch_describe": (_i, [_p, ctypes.c_char_p, _i]),
+    "hr_batch_check": (_i, [_p]),
+    "hr_batch_device_bytes": (ctypes.c_size_t, [_p]),
+    "hr_batch_plan_destroy": (None, [_p]),
+    "hr_add_poisson_noise": (_i, [_p, ctypes.c_longlong, _d, ctypes.c_ulonglong, _p]),
+    "hr_cnn_param_count": (ctypes.c_size_t, []),
+    "hr_cnn_create": (_i, [ctypes.POINTER(_p), _p]),
+    "hr_cnn_get_params": (_i, [_p, _p]),
+    "hr_cnn_get_grads": (_i, [_p, _p]),
+    "hr_cnn_train_step": (_i, [_p, _p, _p, _p, _i, _i, _i, _f, _f, _p, _p]),
+    "hr_cnn_forward": (_i, [_p, _p, _p, _p, ctypes.c_longlong, ctypes.c_longlong, _i, _i, _i, _f, _p]),
+    "hr_cnn_apply_volume": (_i, [_p, _p, _p, _i, _i, _i, _f, _i, _p]),
+    "hr_cnn_pack_input": (_i, [_p, _p, _i, _i, _i, _i, _i, _f, _p]),
+    "hr_cnn_check": (_i, [_p]),
+    "hr_cnn_destroy": (None, [_p]),
     "hr_recon_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc)]),
     "hr_recon_execute": (_i, [_p, _p, _p, _p]),
     "hr_recon_execute_host": (_i, [_p, _p, _p]),

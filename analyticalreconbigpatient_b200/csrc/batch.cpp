@@ -1,0 +1,300 @@
+// Several helical scans of uneven length in one persistent backprojection launch.
+//
+// Each scan is the per-segment sequence of src/analyticalReconBigPatient.m:77-146
+// (rebin, drop the overlap, filter, backproject). Rebinning and the tensor-core
+// filter run scan after scan through one shared rebinned buffer and one shared
+// split-operand scratch; every scan keeps its own BF16 filtered data, and one
+// persistent launch then backprojects the (scan, z block, column tile) items of
+// all scans, so small scans fill the GPU together instead of each leaving a tail.
+// The sequence is captured into a CUDA graph for the buffer addresses it is
+// given and replayed while they stay the same.
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "hr_internal.h"
+#include "bp_fast.h"
+
+struct hr_batch_plan {
+  int n = 0;
+  std::vector<hr_recon_desc> d;
+  std::vector<hr_rebin_plan*> rebin;
+  std::vector<hr_filter_tc_plan*> ftc;
+  std::vector<hr_bp_plan*> bp;
+  std::vector<uint32_t*> pairs;  // per scan: [PN][ZL][YL] BF16 channel pairs
+  std::vector<int> nz;           // per scan: slices per thread of its backprojection
+  float* d_rebinned = nullptr;   // shared: the largest scan's [ViewN][YL][ZL]
+  void* d_split[3] = {};         // shared tensor-core filter operands
+  int variant = 0, tuned = 0;
+  int ctas[hr::kBatchVariants_n] = {};
+  float tuned_ms[hr::kBatchVariants_n] = {};
+  cudaStream_t sc = nullptr;  // capture stream
+  cudaGraphExec_t graph = nullptr;
+  std::vector<const void*> graph_ptrs;
+  int graph_variant = -1;
+  size_t bytes = 0;
+};
+
+namespace {
+
+void destroy(hr_batch_plan* p) {
+  if (!p) return;
+  if (p->graph) cudaGraphExecDestroy(p->graph);
+  for (auto* r : p->rebin) hr_rebin_plan_destroy(r);
+  for (auto* f : p->ftc) hr_filter_tc_plan_destroy(f);
+  for (auto* b : p->bp) hr_bp_plan_destroy(b);
+  for (auto* q : p->pairs) cudaFree(q);
+  cudaFree(p->d_rebinned);
+  for (void* q : p->d_split) cudaFree(q);
+  if (p->sc) cudaStreamDestroy(p->sc);
+  delete p;
+}
+
+int alloc(hr_batch_plan* p, void** ptr, size_t bytes) {
+  HR_CUDA_TRY(cudaMalloc(ptr, bytes));
+  p->bytes += bytes;
+  return HR_OK;
+}
+
+int scans_of(const hr_batch_plan* p, float* const* vols, std::vector<hr::BpFastBatchScan>* out) {
+  out->resize(p->n);
+  for (int i = 0; i < p->n; ++i) {
+    hr::BpFastBatchScan& b = (*out)[i];
+    HR_TRY(hr::bp_plan_fast_parts(p->bp[i], &b.g, &b.f));
+    b.vol = vols[i];
+    b.fpb = p->pairs[i];
+    b.nz = p->nz[i];
+  }
+  return HR_OK;
+}
+
+int enqueue(const hr_batch_plan* p, float* const* vols, const float* const* fans, cudaStream_t s) {
+  for (int i = 0; i < p->n; ++i) {
+    HR_TRY(hr_rebin_execute(p->rebin[i], p->d_rebinned, fans[i], s));
+    HR_TRY(hr_filter_tc_execute(p->ftc[i], p->pairs[i], p->d_rebinned, HR_LAYOUT_REBIN, p->d[i].view0, s));
+  }
+  std::vector<hr::BpFastBatchScan> sc;
+  HR_TRY(scans_of(p, vols, &sc));
+  const long long items = hr::bp_fast_batch_items(sc.data(), p->n);
+  return hr::bp_fast_batch_execute(sc.data(), p->n, p->variant, 0, (int)items, p->ctas[p->variant], s);
+}
+
+// Picks each scan's slices per thread with its own plan's autotuner (the
+// fastest per-slice variant on a band of its slices), then times every batch
+// variant on the whole batch and keeps the fastest. Backprojects into scratch
+// volumes. HELIXRECON_BATCH_VARIANT=<index> pins the batch variant (the
+// per-scan choice still runs).
+int autotune(hr_batch_plan* p) {
+  size_t total = 0;
+  std::vector<size_t> off(p->n);
+  for (int i = 0; i < p->n; ++i) {
+    off[i] = total;
+    total += (size_t)p->d[i].bp.XN * p->d[i].bp.YN * p->d[i].bp.ZN;
+  }
+  hr::DeviceBuffer tmp;
+  HR_TRY(tmp.alloc(total * sizeof(float)));
+  std::vector<float*> vols(p->n);
+  for (int i = 0; i < p->n; ++i) {
+    vols[i] = tmp.as<float>() + off[i];
+    HR_CUDA_TRY(cudaMemsetAsync(p->pairs[i], 0,
+                                sizeof(uint32_t) * (size_t)p->d[i].bp.PN * p->d[i].ZL * p->d[i].YL, p->sc));
+  }
+  p->nz.assign(p->n, 8);
+  for (int i = 0; i < p->n; ++i) {
+    HR_TRY(hr_bp_autotune(p->bp[i], vols[i], p->pairs[i], p->sc));
+    const hr::BpFastGeom* g;
+    const hr::BpFast* f;
+    HR_TRY(hr::bp_plan_fast_parts(p->bp[i], &g, &f));
+    p->nz[i] = hr::bp_fast_best_per_slice_nz(*f);
+  }
+  const char* pin = std::getenv("HELIXRECON_BATCH_VARIANT");
+  if (pin && *pin) {
+    char* end = nullptr;
+    const long v = std::strtol(pin, &end, 10);
+    HR_REQUIRE(*end == '\0' && v >= 0 && v < hr::kBatchVariants_n,
+               "HELIXRECON_BATCH_VARIANT must be an integer in [0, %d)", hr::kBatchVariants_n);
+    p->variant = (int)v;
+    p->tuned = 2;
+    return HR_OK;
+  }
+  std::vector<hr::BpFastBatchScan> sc;
+  HR_TRY(scans_of(p, vols.data(), &sc));
+  const long long items = hr::bp_fast_batch_items(sc.data(), p->n);
+  cudaEvent_t e0, e1;
+  HR_CUDA_TRY(cudaEventCreate(&e0));
+  HR_CUDA_TRY(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_v = 0, st = HR_OK;
+  for (int v = 0; v < hr::kBatchVariants_n && st == HR_OK; ++v) {
+    float ms = 1e30f;
+    for (int rep = 0; rep < 2 && st == HR_OK; ++rep) {
+      cudaEventRecord(e0, p->sc);
+      st = hr::bp_fast_batch_execute(sc.data(), p->n, v, 0, (int)items, p->ctas[v], p->sc);
+      cudaEventRecord(e1, p->sc);
+      if (cudaEventSynchronize(e1) != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "batch autotune: launch failed");
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep > 0) ms = t;
+    }
+    p->tuned_ms[v] = ms;
+    if (ms < best) {
+      best = ms;
+      best_v = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != HR_OK) return st;
+  p->variant = best_v;
+  p->tuned = 1;
+  return HR_OK;
+}
+
+}  // namespace
+
+extern "C" int hr_batch_plan_create(hr_batch_plan** plan, const hr_recon_desc* descs, int n) {
+  hr::clear_error();
+  HR_REQUIRE(plan != nullptr && descs != nullptr, "hr_batch_plan_create: NULL argument");
+  *plan = nullptr;
+  HR_REQUIRE(n >= 1 && n <= hr::kBatchMaxScans, "hr_batch_plan_create: %d scans (1..%d)", n, hr::kBatchMaxScans);
+  for (int i = 0; i < n; ++i) {
+    const hr_recon_desc& d = descs[i];
+    HR_REQUIRE(d.w != nullptr, "hr_batch_plan_create: scan %d has no weight table", i);
+    HR_REQUIRE(d.form == HR_FORM_FAST, "hr_batch_plan_create: scan %d: the batch runs the fast form only", i);
+    HR_REQUIRE(d.bp.YL == d.YL && d.bp.ZL == d.ZL, "hr_batch_plan_create: scan %d: bp.YL/ZL differ from YL/ZL", i);
+    HR_REQUIRE(d.view0 >= 0 && d.view0 + d.bp.PN <= d.ViewN,
+               "hr_batch_plan_create: scan %d: views [%d, %d) exceed the %d rebinned views", i, d.view0,
+               d.view0 + d.bp.PN, d.ViewN);
+  }
+  HR_TRY(hr::require_device());
+  hr_batch_plan* p = new hr_batch_plan;
+  p->n = n;
+  p->d.assign(descs, descs + n);
+  size_t nfan_max = 0, split_max = 0;
+  for (int i = 0; i < n; ++i) {
+    p->d[i].w = nullptr;
+    nfan_max = std::max(nfan_max, (size_t)descs[i].YL * descs[i].ZL * descs[i].ViewN);
+    split_max = std::max(split_max, hr::filter_tc_scratch_bytes(descs[i].YL, descs[i].ZL, descs[i].bp.PN));
+  }
+  int st = alloc(p, (void**)&p->d_rebinned, nfan_max * sizeof(float));
+  for (int k = 0; k < 3 && st == HR_OK; ++k) st = alloc(p, &p->d_split[k], split_max);
+  for (int i = 0; i < n && st == HR_OK; ++i) {
+    const hr_recon_desc& d = descs[i];
+    hr_rebin_plan* r = nullptr;
+    hr_filter_tc_plan* f = nullptr;
+    hr_bp_plan* b = nullptr;
+    uint32_t* q = nullptr;
+    st = hr_rebin_plan_create(&r, d.YL, d.ZL, d.ViewN, d.YLC, d.dYA, d.DeltaTheta, d.PLC, d.DeltaT, d.DeltaFai,
+                              d.SO);
+    p->rebin.push_back(r);
+    if (st == HR_OK)
+      st = hr::filter_tc_create_shared(&f, d.YL, d.ZL, d.bp.PN, d.fPLC, d.fZLC, d.fdYL, d.fdZL, d.fSO, p->d_split);
+    p->ftc.push_back(f);
+    if (st == HR_OK) st = hr_bp_plan_create(&b, &d.bp, d.w, HR_FORM_FAST);
+    p->bp.push_back(b);
+    if (st == HR_OK) st = alloc(p, (void**)&q, sizeof(uint32_t) * (size_t)d.bp.PN * d.ZL * d.YL);
+    p->pairs.push_back(q);
+  }
+  for (int v = 0; v < hr::kBatchVariants_n && st == HR_OK; ++v) st = hr::bp_fast_batch_grid(v, &p->ctas[v]);
+  if (st == HR_OK) {
+    const cudaError_t e = cudaStreamCreateWithFlags(&p->sc, cudaStreamNonBlocking);
+    if (e != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "hr_batch_plan_create: %s", cudaGetErrorString(e));
+  }
+  if (st == HR_OK) st = autotune(p);
+  if (st != HR_OK) {
+    destroy(p);
+    return st;
+  }
+  *plan = p;
+  return HR_OK;
+}
+
+extern "C" int hr_batch_execute(hr_batch_plan* p, float* const* d_vols, const float* const* d_fans, void* stream) {
+  HR_REQUIRE(p != nullptr && d_vols != nullptr && d_fans != nullptr, "hr_batch_execute: NULL argument");
+  std::vector<const void*> ptrs;
+  for (int i = 0; i < p->n; ++i) {
+    HR_REQUIRE(d_vols[i] != nullptr && d_fans[i] != nullptr, "hr_batch_execute: NULL buffer for scan %d", i);
+    ptrs.push_back(d_vols[i]);
+    ptrs.push_back(d_fans[i]);
+  }
+  cudaStream_t s = hr::as_stream(stream);
+  if (!p->graph || ptrs != p->graph_ptrs || p->graph_variant != p->variant) {
+    if (p->graph) cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
+    cudaGraph_t gr = nullptr;
+    HR_CUDA_TRY(cudaStreamBeginCapture(p->sc, cudaStreamCaptureModeRelaxed));
+    const int st = enqueue(p, d_vols, d_fans, p->sc);
+    const cudaError_t e = cudaStreamEndCapture(p->sc, &gr);
+    if (st != HR_OK || e != cudaSuccess) {
+      if (gr) cudaGraphDestroy(gr);
+      return st != HR_OK ? st : hr::fail(HR_ERR_CUDA, "hr_batch_execute: capture failed: %s", cudaGetErrorString(e));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&p->graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (ei != cudaSuccess) {
+      p->graph = nullptr;
+      return hr::fail(HR_ERR_CUDA, "hr_batch_execute: graph instantiation failed: %s", cudaGetErrorString(ei));
+    }
+    p->graph_ptrs = ptrs;
+    p->graph_variant = p->variant;
+  }
+  HR_CUDA_TRY(cudaGraphLaunch(p->graph, s));
+  return HR_OK;
+}
+
+extern "C" int hr_batch_backproject(hr_batch_plan* p, float* const* d_vols, void* stream) {
+  HR_REQUIRE(p != nullptr && d_vols != nullptr, "hr_batch_backproject: NULL argument");
+  for (int i = 0; i < p->n; ++i) HR_REQUIRE(d_vols[i] != nullptr, "hr_batch_backproject: NULL volume %d", i);
+  std::vector<hr::BpFastBatchScan> sc;
+  HR_TRY(scans_of(p, d_vols, &sc));
+  const long long items = hr::bp_fast_batch_items(sc.data(), p->n);
+  return hr::bp_fast_batch_execute(sc.data(), p->n, p->variant, 0, (int)items, p->ctas[p->variant],
+                                   hr::as_stream(stream));
+}
+
+extern "C" int hr_batch_select(hr_batch_plan* p, int variant) {
+  HR_REQUIRE(p != nullptr, "hr_batch_select: NULL plan");
+  HR_REQUIRE(variant >= 0 && variant < hr::kBatchVariants_n, "hr_batch_select: variant %d out of range [0, %d)",
+             variant, hr::kBatchVariants_n);
+  p->variant = variant;
+  return HR_OK;
+}
+
+extern "C" int hr_batch_describe(const hr_batch_plan* p, char* buf, int len) {
+  HR_REQUIRE(p != nullptr, "hr_batch_describe: NULL plan");
+  if (!buf || len <= 0) return HR_OK;
+  std::vector<float*> vols(p->n, nullptr);
+  std::vector<hr::BpFastBatchScan> sc;
+  HR_TRY(scans_of(p, vols.data(), &sc));
+  int k = snprintf(buf, (size_t)len, "%d scans, %lld work items in one persistent launch of %d CTAs (>= %d per SM); "
+                   "slices per thread by scan:", p->n, hr::bp_fast_batch_items(sc.data(), p->n),
+                   p->ctas[p->variant], hr::kBatchVariants[p->variant].min_ctas);
+  for (int i = 0; i < p->n && k > 0 && k < len; ++i) k += snprintf(buf + k, (size_t)(len - k), " %d", p->nz[i]);
+  if (k > 0 && k < len)
+    k += snprintf(buf + k, (size_t)(len - k), " %s",
+                  p->tuned == 2 ? "(pinned by HELIXRECON_BATCH_VARIANT)"
+                  : p->tuned ? "(autotuned; batch ms:" : "(selected)");
+  if (p->tuned == 1) {
+    for (int v = 0; v < hr::kBatchVariants_n && k > 0 && k < len; ++v)
+      k += snprintf(buf + k, (size_t)(len - k), " v%d=%.2f", v, p->tuned_ms[v]);
+    if (k > 0 && k < len) snprintf(buf + k, (size_t)(len - k), ")");
+  }
+  return HR_OK;
+}
+
+extern "C" int hr_batch_check(const hr_batch_plan* p) {
+  HR_REQUIRE(p != nullptr, "hr_batch_check: NULL plan");
+  for (auto* f : p->ftc) HR_TRY(hr_filter_tc_check(f));
+  return HR_OK;
+}
+
+extern "C" size_t hr_batch_device_bytes(const hr_batch_plan* p) {
+  if (!p) return 0;
+  size_t b = p->bytes;
+  for (auto* f : p->ftc) b += hr_filter_tc_device_bytes(f);
+  return b;
+}
+
+extern "C" void hr_batch_plan_destroy(hr_batch_plan* p) { destroy(p); }

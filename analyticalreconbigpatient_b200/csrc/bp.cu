@@ -356,6 +356,13 @@ extern "C" int hr_bp_execute(const hr_bp_plan* pl, void* d_vol, const void* d_fp
   return HR_OK;
 }
 
+int hr::bp_plan_fast_parts(const hr_bp_plan* pl, const BpFastGeom** g, const BpFast** f) {
+  HR_REQUIRE(pl != nullptr && pl->form == HR_FORM_FAST, "backprojection plan is not of the fast form");
+  *g = &pl->fg;
+  *f = &pl->fast;
+  return HR_OK;
+}
+
 extern "C" int hr_bp_autotune(hr_bp_plan* pl, void* d_vol, const void* d_fp, void* stream) {
   HR_REQUIRE(pl != nullptr && d_vol != nullptr && d_fp != nullptr, "hr_bp_autotune: NULL argument");
   if (pl->form != HR_FORM_FAST) return HR_OK;

@@ -102,20 +102,24 @@ __device__ __forceinline__ float blend(uint32_t w0, uint32_t w1, float fu, float
 // whose 2*CH gathers are then issued together (addresses clamped into the
 // detector, out-of-detector or out-of-window slices weighted by 0), and only
 // then consumed -- more loads in flight per warp at the cost of registers.
+// Per-scan table pointers of the fast backprojection.
+struct ZTabs {
+  const float2* trig;     // per view: {cos, sin}
+  const float2* ztab;     // per z block and view of its window: NZ x {t2, Q}
+  const uint32_t* zmask;  // per z block and view: slices whose window holds the view
+  const int2* zblock;     // per z block: {first view, number of views}
+  const int* zoff;        // per z block: table row of its first view
+};
+
 template <int NZ, int CH>
-__global__ void __launch_bounds__(kBx* kBy) bp_fast_kernel(float* __restrict__ vol, const uint32_t* __restrict__ fpb,
-                                                          const float2* __restrict__ trig,
-                                                          const float2* __restrict__ ztab,
-                                                          const uint32_t* __restrict__ zmask,
-                                                          const int2* __restrict__ zblock,
-                                                          const int* __restrict__ zoff, FastParams P, int b_first) {
-  const int xi = blockIdx.x * kBx + threadIdx.x;
-  const int yi = blockIdx.y * kBy + threadIdx.y;
-  const int b = b_first + blockIdx.z;
+__device__ __forceinline__ void fast_column(float* __restrict__ vol, const uint32_t* __restrict__ fpb,
+                                            const ZTabs& T, const FastParams& P, int xi, int yi, int b) {
+  const float2* __restrict__ trig = T.trig;
+  const float2* __restrict__ ztab = T.ztab;
+  const uint32_t* __restrict__ zmask = T.zmask;
   const int z0 = b * NZ;
-  if (xi >= P.XN || yi >= P.YN) return;
-  const int2 blk = zblock[b];  // {first view, number of views} of the block's union window
-  const int off = zoff[b];     // row of the block's first view in the table
+  const int2 blk = T.zblock[b];  // {first view, number of views} of the block's union window
+  const int off = T.zoff[b];     // row of the block's first view in the table
   const float x = ((float)xi - P.XNC) * P.dx;
   const float y = ((float)yi - P.YNC) * P.dy;
   float res[NZ];
@@ -220,22 +224,15 @@ __device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
 // window test is one uniform branch per pair. Same operations per (voxel,
 // view) as bp_fast_kernel, in the same view order.
 template <int NZ>
-__global__ void __launch_bounds__(kBx* kBy) bp_fast_pair_kernel(float* __restrict__ vol,
-                                                               const uint32_t* __restrict__ fpb,
-                                                               const float2* __restrict__ trig,
-                                                               const float2* __restrict__ ztab,
-                                                               const uint32_t* __restrict__ zmask,
-                                                               const int2* __restrict__ zblock,
-                                                               const int* __restrict__ zoff, FastParams P,
-                                                               int b_first) {
+__device__ __forceinline__ void fast_column_pairs(float* __restrict__ vol, const uint32_t* __restrict__ fpb,
+                                                  const ZTabs& T, const FastParams& P, int xi, int yi, int b) {
   static_assert(NZ % 2 == 0, "slices are processed in pairs");
-  const int xi = blockIdx.x * kBx + threadIdx.x;
-  const int yi = blockIdx.y * kBy + threadIdx.y;
-  const int b = b_first + blockIdx.z;
+  const float2* __restrict__ trig = T.trig;
+  const float2* __restrict__ ztab = T.ztab;
+  const uint32_t* __restrict__ zmask = T.zmask;
   const int z0 = b * NZ;
-  if (xi >= P.XN || yi >= P.YN) return;
-  const int2 blk = zblock[b];
-  const int off = zoff[b];
+  const int2 blk = T.zblock[b];
+  const int off = T.zoff[b];
   const float x = ((float)xi - P.XNC) * P.dx;
   const float y = ((float)yi - P.YNC) * P.dy;
   uint64_t res[NZ / 2];
@@ -298,6 +295,71 @@ __global__ void __launch_bounds__(kBx* kBy) bp_fast_pair_kernel(float* __restric
     up2(res[c], a, bb);
     if (z0 + 2 * c < P.ZN) out[2 * c] = a * P.DeltaFai;
     if (z0 + 2 * c + 1 < P.ZN) out[2 * c + 1] = bb * P.DeltaFai;
+  }
+}
+
+// CH >= 0: fast_column<NZ, CH>; CH < 0: slice pairs in packed FP32x2.
+template <int NZ, int CH>
+__device__ __forceinline__ void column(float* vol, const uint32_t* fpb, const ZTabs& T, const FastParams& P, int xi,
+                                       int yi, int b) {
+  if constexpr (CH < 0)
+    fast_column_pairs<NZ>(vol, fpb, T, P, xi, yi, b);
+  else
+    fast_column<NZ, CH>(vol, fpb, T, P, xi, yi, b);
+}
+
+// One CTA per (8 x 16 column tile, z block); grid z covers z blocks
+// [b_first, b_first + gridDim.z).
+template <int NZ, int CH>
+__global__ void __launch_bounds__(kBx* kBy) bp_fast_kernel(float* __restrict__ vol, const uint32_t* __restrict__ fpb,
+                                                          const ZTabs T, const FastParams P, int b_first) {
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  if (xi >= P.XN || yi >= P.YN) return;
+  column<NZ, CH>(vol, fpb, T, P, xi, yi, b_first + blockIdx.z);
+}
+
+// Several scans of uneven size in one persistent launch. Work items are
+// (scan, z block, column tile), numbered scan by scan with the column tile
+// fastest, and dealt to the resident CTAs round robin (items that run
+// together share a z block and so its views in L2). Each scan keeps the
+// slices per thread its own geometry favours (16, 8 or 4: a uniform branch
+// per item).
+struct BatchScan {
+  FastParams P;
+  ZTabs T;
+  float* vol;
+  const uint32_t* fpb;
+  int tiles_x, tiles_y, item0, nz;
+};
+struct BatchParams {
+  BatchScan s[hr::kBatchMaxScans];
+  int n;
+  int begin, count;  // items [begin, begin + count)
+  int grid;          // CTAs launched
+};
+
+// MB: CTAs per SM the register allocation must allow (1: no constraint).
+template <int MB>
+__global__ void __launch_bounds__(kBx* kBy, MB) bp_fast_batch_kernel(const __grid_constant__ BatchParams B) {
+  for (int k = blockIdx.x; k < B.count; k += gridDim.x) {
+    const int item = B.begin + k;
+    int sc = 0;
+    while (sc + 1 < B.n && item >= B.s[sc + 1].item0) ++sc;
+    const BatchScan& S = B.s[sc];
+    const int local = item - S.item0;
+    const int t = local / S.tiles_x;
+    const int xi = (local - t * S.tiles_x) * kBx + threadIdx.x;
+    const int yi = (t % S.tiles_y) * kBy + threadIdx.y;
+    const int b = t / S.tiles_y;
+    if (xi < S.P.XN && yi < S.P.YN) {
+      if (S.nz == 16)
+        column<16, 0>(S.vol, S.fpb, S.T, S.P, xi, yi, b);
+      else if (S.nz == 8)
+        column<8, 0>(S.vol, S.fpb, S.T, S.P, xi, yi, b);
+      else
+        column<4, 0>(S.vol, S.fpb, S.T, S.P, xi, yi, b);
+    }
   }
 }
 
@@ -475,22 +537,15 @@ static FastParams make_params(const BpFastGeom& g) {
   return P;
 }
 
+static ZTabs ztabs(const BpFastTables& t, const BpFast& f) {
+  return ZTabs{f.d_trig, t.d_tab, t.d_mask, reinterpret_cast<const int2*>(t.d_zblock), t.d_zblock + 2 * t.nblocks};
+}
+
 template <int NZ, int CH>
 static void launch_variant(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol,
                            const uint32_t* fpb, int b_first, int b_count, cudaStream_t s) {
   dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
-  bp_fast_kernel<NZ, CH><<<grid, dim3(kBx, kBy), 0, s>>>(vol, fpb, f.d_trig, t.d_tab, t.d_mask,
-                                                          reinterpret_cast<const int2*>(t.d_zblock),
-                                                          t.d_zblock + 2 * t.nblocks, P, b_first);
-}
-
-template <int NZ>
-static void launch_pair_variant(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol,
-                                const uint32_t* fpb, int b_first, int b_count, cudaStream_t s) {
-  dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
-  bp_fast_pair_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, fpb, f.d_trig, t.d_tab, t.d_mask,
-                                                           reinterpret_cast<const int2*>(t.d_zblock),
-                                                           t.d_zblock + 2 * t.nblocks, P, b_first);
+  bp_fast_kernel<NZ, CH><<<grid, dim3(kBx, kBy), 0, s>>>(vol, fpb, ztabs(t, f), P, b_first);
 }
 
 // Launches variant v over z blocks [b_first, b_first + b_count) (count < 0: all).
@@ -509,10 +564,10 @@ static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, 
     case 3: launch_variant<8, 0>(t, f, P, vol, fpb, b_first, b_count, s); break;
     case 4: launch_variant<8, 4>(t, f, P, vol, fpb, b_first, b_count, s); break;
     case 5: launch_variant<8, 8>(t, f, P, vol, fpb, b_first, b_count, s); break;
-    case 6: launch_pair_variant<16>(t, f, P, vol, fpb, b_first, b_count, s); break;
-    case 7: launch_pair_variant<8>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 6: launch_variant<16, -1>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 7: launch_variant<8, -1>(t, f, P, vol, fpb, b_first, b_count, s); break;
     case 8: launch_variant<4, 0>(t, f, P, vol, fpb, b_first, b_count, s); break;
-    case 9: launch_pair_variant<4>(t, f, P, vol, fpb, b_first, b_count, s); break;
+    case 9: launch_variant<4, -1>(t, f, P, vol, fpb, b_first, b_count, s); break;
     case 10: launch_variant<4, 4>(t, f, P, vol, fpb, b_first, b_count, s); break;
     default: return hr::fail(HR_ERR_INVALID_ARGUMENT, "fast backprojection: unknown variant %d", v);
   }
@@ -520,12 +575,95 @@ static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, 
   return HR_OK;
 }
 
+static int table_of_nz(int nz) {
+  for (int i = 0; i < kFastTableSets; ++i)
+    if (kFastNz[i] == nz) return i;
+  return -1;
+}
+
+long long bp_fast_batch_items(const BpFastBatchScan* scans, int n) {
+  long long total = 0;
+  for (int i = 0; i < n; ++i) {
+    const BpFastGeom& g = *scans[i].g;
+    const int ts = table_of_nz(scans[i].nz);
+    if (ts < 0) return -1;
+    total += (long long)((g.XN + kBx - 1) / kBx) * ((g.YN + kBy - 1) / kBy) * scans[i].f->t[ts].nblocks;
+  }
+  return total;
+}
+
+template <int MB>
+static int batch_launch(const BatchParams* B, int* ctas, cudaStream_t s) {
+  if (ctas) {
+    int per_sm = 0;
+    HR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_fast_batch_kernel<MB>, kBx * kBy, 0));
+    *ctas = std::max(per_sm, 1) * sm_count();
+    return HR_OK;
+  }
+  bp_fast_batch_kernel<MB><<<B->grid, dim3(kBx, kBy), 0, s>>>(*B);
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
+// ctas != nullptr: report the resident CTAs of batch variant bv; else launch *B.
+static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t s) {
+  switch (bv) {
+    case 0: return batch_launch<1>(B, ctas, s);
+    case 1: return batch_launch<10>(B, ctas, s);
+    case 2: return batch_launch<12>(B, ctas, s);
+    default: return hr::fail(HR_ERR_INVALID_ARGUMENT, "batch backprojection: unknown variant %d", bv);
+  }
+}
+
+int bp_fast_batch_grid(int bv, int* ctas) { return batch_dispatch(bv, nullptr, ctas, nullptr); }
+
+int bp_fast_batch_execute(const BpFastBatchScan* scans, int n, int bv, int begin, int count, int ctas,
+                          cudaStream_t s) {
+  HR_REQUIRE(n >= 1 && n <= kBatchMaxScans, "batch backprojection: %d scans (1..%d per launch)", n, kBatchMaxScans);
+  HR_REQUIRE(bv >= 0 && bv < kBatchVariants_n, "batch backprojection: unknown variant %d", bv);
+  HR_REQUIRE(ctas >= 1, "batch backprojection: no CTAs");
+  BatchParams B{};
+  long long item0 = 0;
+  for (int i = 0; i < n; ++i) {
+    const BpFastGeom& g = *scans[i].g;
+    const int ts = table_of_nz(scans[i].nz);
+    HR_REQUIRE(ts >= 0, "batch backprojection: scan %d: %d slices per thread is not a table set", i, scans[i].nz);
+    const BpFastTables& t = scans[i].f->t[ts];
+    BatchScan& S = B.s[i];
+    S.P = make_params(g);
+    S.T = ztabs(t, *scans[i].f);
+    S.vol = scans[i].vol;
+    S.fpb = scans[i].fpb;
+    S.tiles_x = (g.XN + kBx - 1) / kBx;
+    S.tiles_y = (g.YN + kBy - 1) / kBy;
+    S.item0 = (int)item0;
+    S.nz = scans[i].nz;
+    item0 += (long long)S.tiles_x * S.tiles_y * t.nblocks;
+  }
+  HR_REQUIRE(item0 < (1ll << 31), "batch backprojection: too many work items");
+  HR_REQUIRE(begin >= 0 && count >= 0 && (long long)begin + count <= item0,
+             "batch backprojection: items [%d, %d) outside [0, %lld)", begin, begin + count, item0);
+  B.n = n;
+  B.begin = begin;
+  B.count = count;
+  B.grid = std::min(ctas, std::max(count, 1));
+  if (count == 0) return HR_OK;
+  return batch_dispatch(bv, &B, nullptr, s);
+}
+
+int bp_fast_best_per_slice_nz(const BpFast& f) {
+  // per-slice variants of each table set: 0 (16), 3 (8), 8 (4)
+  const int cand[3] = {0, 3, 8};
+  int best = 3;
+  for (int v : cand)
+    if (f.tuned == 1 && f.tuned_ms[v] < f.tuned_ms[best]) best = v;
+  return kFastNz[kFastVariants[best].table];
+}
+
 int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s) {
   return run_variant(f, g, f.variant, vol, fpb, 0, -1, s);
 }
 
-// Times every variant on the same middle band of 32 slices (all columns) and
-// keeps the fastest. The band is written into vol; synchronises the stream.
 // HELIXRECON_BP_VARIANT=<index> pins the variant and skips the timing (for
 // profiling runs, whose serialised launches would skew the choice, and for
 // reproducible benchmarks).
@@ -538,6 +676,8 @@ static int pinned_variant() {
   return (int)v;
 }
 
+// Times every variant on the same middle band of 32 slices (all columns) and
+// keeps the fastest. The band is written into vol; synchronises the stream.
 int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s) {
   const int pin = pinned_variant();
   HR_REQUIRE(pin != -2, "HELIXRECON_BP_VARIANT must be an integer in [0, %d)", kFastVariants_n);

@@ -7,6 +7,8 @@
 #include <cstdint>
 #include <vector>
 
+struct hr_bp_plan;
+
 namespace hr {
 
 struct BpFastGeom {
@@ -31,6 +33,10 @@ constexpr FastVariant kFastVariants[] = {{0, 0}, {0, 4}, {0, 8}, {1, 0}, {1, 4},
                                          {0, -1}, {1, -1}, {2, 0}, {2, -1}, {2, 4}};
 constexpr int kFastVariants_n = sizeof(kFastVariants) / sizeof(kFastVariants[0]);
 constexpr int kFastDefaultVariant = 0;
+
+// Scans one persistent batch launch covers (their descriptors travel as one
+// kernel parameter block).
+constexpr int kBatchMaxScans = 16;
 
 struct BpFastTables {
   int nz = 0, nblocks = 0;
@@ -76,6 +82,32 @@ void bp_fast_destroy(BpFast* f);
 int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s);
 int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s);
 int bp_fast_describe(const BpFast& f, char* buf, int len);
+// Several scans in one persistent launch. Each scan runs the per-slice kernel
+// body with its own slices per thread (16, 8 or 4); batch variants differ in
+// the CTAs per SM their registers must allow (1: unconstrained; 10; 12).
+struct BatchVariant {
+  int min_ctas;
+};
+constexpr BatchVariant kBatchVariants[] = {{1}, {10}, {12}};
+constexpr int kBatchVariants_n = sizeof(kBatchVariants) / sizeof(kBatchVariants[0]);
+struct BpFastBatchScan {
+  const BpFast* f;
+  const BpFastGeom* g;
+  float* vol;
+  const uint32_t* fpb;
+  int nz;  // slices per thread (a table set)
+};
+// Work items (scan, z block, 8 x 16 column tile) of the batch (-1: a bad nz).
+long long bp_fast_batch_items(const BpFastBatchScan* scans, int n);
+// Persistent CTAs a launch of batch variant bv keeps resident (occupancy x SMs).
+int bp_fast_batch_grid(int bv, int* ctas);
+// Backprojects items [begin, begin + count) of the batch with at most ctas CTAs.
+int bp_fast_batch_execute(const BpFastBatchScan* scans, int n, int bv, int begin, int count, int ctas,
+                          cudaStream_t s);
+// Slices per thread of the fastest per-slice variant the plan's autotuner timed (8 if untuned).
+int bp_fast_best_per_slice_nz(const BpFast& f);
+// The fast-form geometry and tables of a backprojection plan (HR_FORM_FAST).
+int bp_plan_fast_parts(const hr_bp_plan* plan, const BpFastGeom** g, const BpFast** f);
 // FP32 rows [rows][YL] -> BF16 channel pairs: word u = bf16(x[u]) | bf16(x[u+1]) << 16.
 int pack_pairs(uint32_t* out, const float* in, long long rows, int YL, cudaStream_t s);
 

@@ -359,21 +359,24 @@ struct hr_filter_tc_plan {
   int* d_err;
   CUtensorMap m_a[kParts], m_t[kParts];
   size_t bytes;
+  bool owns_a;  // false: the split parts live in a caller's scratch
 };
 
 static void tc_destroy(hr_filter_tc_plan* p) {
   if (!p) return;
   for (int i = 0; i < kParts; ++i) {
-    cudaFree(p->d_a[i]);
+    if (p->owns_a) cudaFree(p->d_a[i]);
     cudaFree(p->d_t[i]);
   }
   cudaFree(p->d_err);
   delete p;
 }
 
-extern "C" int hr_filter_tc_plan_create(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC,
-                                        float dYL, float dZL, float SO) {
-  hr::clear_error();
+// ext: three scratch buffers of at least filter_tc_scratch_bytes(YL, ZL, ViewN)
+// bytes each for the split parts (shared between plans that run one after the
+// other), or nullptr to allocate them in the plan.
+static int tc_create(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC, float dYL, float dZL,
+                     float SO, void* const* ext) {
   HR_REQUIRE(plan != nullptr, "hr_filter_tc_plan_create: plan is NULL");
   *plan = nullptr;
   HR_REQUIRE(YL > 1 && ZL > 0 && ViewN > 0, "tensor-core filter: invalid sizes (YL=%d ZL=%d ViewN=%d)", YL, ZL,
@@ -391,6 +394,7 @@ extern "C" int hr_filter_tc_plan_create(hr_filter_tc_plan** plan, int YL, int ZL
   hr_filter_tc_plan* p = new hr_filter_tc_plan{};
   p->YL = YL; p->ZL = ZL; p->ViewN = ViewN; p->PLC = PLC; p->ZLC = ZLC; p->dYL = dYL; p->dZL = dZL; p->SO = SO;
   p->rows = rows;
+  p->owns_a = ext == nullptr;
   p->KP = (YL + kBK - 1) / kBK * kBK;
   p->n_tiles = (YL + kBNOut - 1) / kBNOut;
   p->TR = p->n_tiles * kBNOut + (kBN - kBNOut);
@@ -412,7 +416,10 @@ extern "C" int hr_filter_tc_plan_create(hr_filter_tc_plan** plan, int YL, int ZL
   int st = HR_OK;
   cudaError_t e = cudaMalloc(&p->d_err, sizeof(int));
   for (int i = 0; i < kParts && e == cudaSuccess; ++i) {
-    e = cudaMalloc(&p->d_a[i], abytes);
+    if (ext)
+      p->d_a[i] = static_cast<__nv_bfloat16*>(ext[i]);
+    else
+      e = cudaMalloc(&p->d_a[i], abytes);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_t[i], tbytes);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_t[i], tp[i].data(), tbytes, cudaMemcpyHostToDevice);
   }
@@ -428,9 +435,25 @@ extern "C" int hr_filter_tc_plan_create(hr_filter_tc_plan** plan, int YL, int ZL
     tc_destroy(p);
     return st;
   }
-  p->bytes = kParts * (abytes + tbytes) + sizeof(int);
+  p->bytes = kParts * ((ext ? 0 : abytes) + tbytes) + sizeof(int);
   *plan = p;
   return HR_OK;
+}
+
+size_t hr::filter_tc_scratch_bytes(int YL, int ZL, int ViewN) {
+  return (size_t)ZL * ViewN * ((YL + kBK - 1) / kBK * kBK) * 2;
+}
+
+int hr::filter_tc_create_shared(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC, float dYL,
+                                float dZL, float SO, void* const scratch[3]) {
+  HR_REQUIRE(scratch && scratch[0] && scratch[1] && scratch[2], "tensor-core filter: NULL scratch");
+  return tc_create(plan, YL, ZL, ViewN, PLC, ZLC, dYL, dZL, SO, scratch);
+}
+
+extern "C" int hr_filter_tc_plan_create(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC,
+                                        float dYL, float dZL, float SO) {
+  hr::clear_error();
+  return tc_create(plan, YL, ZL, ViewN, PLC, ZLC, dYL, dZL, SO, nullptr);
 }
 
 extern "C" int hr_filter_tc_execute(const hr_filter_tc_plan* p, uint32_t* d_pairs, const float* d_in, int in_layout,

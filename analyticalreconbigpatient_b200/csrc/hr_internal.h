@@ -65,4 +65,11 @@ struct DeviceBuffer {
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Tensor-core filter plans whose split-operand scratch (three buffers of
+// filter_tc_scratch_bytes each) belongs to the caller and may be shared by
+// plans that execute one after the other on one stream.
+size_t filter_tc_scratch_bytes(int YL, int ZL, int ViewN);
+int filter_tc_create_shared(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC, float dYL,
+                            float dZL, float SO, void* const scratch[3]);
+
 }  // namespace hr

@@ -9,6 +9,7 @@
 // parallel view angle beta - gamma, which is the relation the rebinning
 // inverts (Fai = Theta + asin(t/SO), src/ParallelRebinningCBCurve.cpp:37-39).
 // Row k: the ray rises (k - ZLC0) dZL over the in-plane distance SD.
+#include <algorithm>
 #include <cmath>
 
 #include "hr_internal.h"
@@ -85,6 +86,65 @@ __global__ void __launch_bounds__(256) project_kernel(float* __restrict__ proj, 
   }
 }
 
+// ---- Poisson photon noise ---------------------------------------------------
+// Counter-based stream: draw j of sample i is splitmix64 of a per-sample state,
+// so the result does not depend on the launch shape.
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long& x) {
+  unsigned long long z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double uniform01(unsigned long long& st) {
+  return (double)(splitmix64(st) >> 11) * 0x1.0p-53;  // [0, 1)
+}
+
+// Poisson(lam). lam < 10: multiplication of uniforms (Knuth); otherwise the
+// transformed rejection method with squeeze, PTRS (W. Hoermann, "The
+// transformed rejection method for generating Poisson random variables",
+// Insurance: Mathematics and Economics 12, 1993). Both loops are bounded; their
+// expected iteration counts are lam + 1 < 11 and about 1.1.
+__device__ double poisson(double lam, unsigned long long& st) {
+  if (!(lam > 0.0)) return 0.0;
+  if (lam < 10.0) {
+    const double L = exp(-lam);
+    double prod = uniform01(st);
+    int k = 0;
+    while (prod > L && k < 1000) {
+      prod *= uniform01(st);
+      ++k;
+    }
+    return (double)k;
+  }
+  const double slam = sqrt(lam), loglam = log(lam);
+  const double b = 0.931 + 2.53 * slam;
+  const double a = -0.059 + 0.02483 * b;
+  const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
+  const double vr = 0.9277 - 3.6224 / (b - 2.0);
+  for (int it = 0; it < 1000; ++it) {
+    const double U = uniform01(st) - 0.5;
+    const double V = uniform01(st);
+    const double us = 0.5 - fabs(U);
+    const double k = floor((2.0 * a / us + b) * U + lam + 0.43);
+    if (us >= 0.07 && V <= vr) return k;
+    if (k < 0.0 || (us < 0.013 && V > us)) continue;
+    if (log(V) + log(inv_alpha) - log(a / (us * us) + b) <= -lam + k * loglam - lgamma(k + 1.0)) return k;
+  }
+  return floor(lam + 0.5);  // not reached in practice (acceptance > 0.9 per draw)
+}
+
+// p -> -log(max(N, 1) / I0) with N ~ Poisson(I0 exp(-p)): line integrals with
+// the photon noise of a transmission measurement at I0 photons per ray.
+__global__ void poisson_noise_kernel(float* __restrict__ proj, long long n, double I0, unsigned long long seed) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long st = seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)(i + 1));
+    splitmix64(st);
+    const double N = poisson(I0 * exp(-(double)proj[i]), st);
+    proj[i] = (float)-log(fmax(N, 1.0) / I0);
+  }
+}
+
 }  // namespace
 
 extern "C" int hr_project_ellipsoids(float* d_proj, int YL, int ZL, int ViewN, double SO, double SD, double dYA,
@@ -101,6 +161,17 @@ extern "C" int hr_project_ellipsoids(float* d_proj, int YL, int ZL, int ViewN, d
   dim3 grid((YL * ZL + 255) / 256, ViewN < 65535 ? ViewN : 65535);
   project_kernel<<<grid, 256, smem, hr::as_stream(stream)>>>(d_proj, YL, ZL, ViewN, SO, SD, dYA, YLC0, dZL, ZLC0,
                                                              BetaS, dBeta, h, d_obj, nobj);
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
+extern "C" int hr_add_poisson_noise(float* d_proj, long long n, double I0, unsigned long long seed, void* stream) {
+  hr::clear_error();
+  HR_REQUIRE(d_proj != nullptr || n == 0, "hr_add_poisson_noise: NULL data");
+  HR_REQUIRE(n >= 0 && I0 >= 1.0, "hr_add_poisson_noise: need n >= 0 and I0 >= 1");
+  if (n == 0) return HR_OK;
+  const long long blocks = std::min<long long>((n + 255) / 256, 8LL * hr::sm_count());
+  poisson_noise_kernel<<<(unsigned)blocks, 256, 0, hr::as_stream(stream)>>>(d_proj, n, I0, seed);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
 }

@@ -263,6 +263,33 @@ def config(name: str) -> Scan:
     raise KeyError(name)
 
 
+def batch_scans(seed: int = 6, n: int = 12) -> list[Scan]:
+    """The uneven batch: ``n`` independent scans on the 888-channel detector at
+    984 views/rotation with rotations uniform in 2..30, rows from {16, 32, 64},
+    pitch from {0.5, 0.9375, 1.375} and a 256x256 (1.953 mm) or 512x512
+    (0.9766 mm) grid of 32..400 slices, drawn from a seeded SplitMix64 stream.
+    Slices are 0.625 mm thick, or thinner where the fully sampled z range of a
+    short scan is shorter than the drawn slice count at 0.625 mm, so every
+    slice lies in the fully sampled range."""
+    from .phantom import SplitMix64
+
+    rng = SplitMix64(seed)
+    pick = lambda opts: opts[min(int(rng.uniform() * len(opts)), len(opts) - 1)]
+    out = []
+    for _ in range(n):
+        rot = min(2 + int(rng.uniform() * 29), 30)
+        ZL = pick((16, 32, 64))
+        pitch = pick((0.5, 0.9375, 1.375))
+        N = pick((256, 512))
+        ZN = min(32 + int(rng.uniform() * 369), 400)
+        d = 500.0 / N
+        sc = Scan(ZL=ZL, pitch=pitch, rotations=rot, XN=N, YN=N, ZN=ZN, dx=d, dy=d, dz=0.625)
+        half = math.ceil(sc.N_2pi / 2.0 * sc.HSCoef)
+        span = sc.h * (sc.PN - 2 * half) / sc.N_2pi
+        out.append(replace(sc, dz=min(0.625, span / ZN)))
+    return out
+
+
 def tiny(**kw) -> Scan:
     """A scaled-down scan for CPU-speed tests: same detector geometry family with
     fewer channels, rows and views."""

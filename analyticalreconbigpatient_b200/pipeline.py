@@ -149,6 +149,70 @@ class SlabRecon:
             pass
 
 
+class BatchRecon:
+    """Several independent scans of uneven size; every scan's rebinning and
+    tensor-core filter, then one persistent backprojection launch over all of
+    them, replayed from a CUDA graph (hr_batch_plan in include/helixrecon.h).
+    Fast form only; at most 16 scans."""
+
+    def __init__(self, scans: list[Scan], device: int | torch.device = 0):
+        self.scans = list(scans)
+        self.device = torch.device("cuda", device) if isinstance(device, int) else device
+        self._plan = ctypes.c_void_p()
+        ws = [view_weights(sc) for sc in self.scans]  # alive until the plan has copied them
+        descs = (_lib.ReconDesc * len(self.scans))(*[recon_desc(sc, w, _lib.HR_FORM_FAST)
+                                                    for sc, w in zip(self.scans, ws)])
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().hr_batch_plan_create(ctypes.byref(self._plan), descs, len(self.scans)))
+
+    def run(self, fans: list[torch.Tensor], volumes: list[torch.Tensor], stream=None) -> None:
+        """fans[i]: CUDA float32 [views][YL][ZL]; volumes[i]: CUDA float32 [YN][XN][ZN]."""
+        n = len(self.scans)
+        if len(fans) != n or len(volumes) != n:
+            raise ValueError(f"expected {n} fans and volumes")
+        for sc, f, v in zip(self.scans, fans, volumes):
+            if not (f.is_cuda and v.is_cuda and f.dtype == torch.float32 and v.dtype == torch.float32):
+                raise TypeError("fans and volumes must be CUDA float32 tensors")
+            if tuple(f.shape) != (sc.views, sc.YL, sc.ZL) or tuple(v.shape) != (sc.YN, sc.XN, sc.ZN):
+                raise ValueError("fan or volume shape does not match its scan")
+        fp = (ctypes.c_void_p * n)(*[f.data_ptr() for f in fans])
+        vp = (ctypes.c_void_p * n)(*[v.data_ptr() for v in volumes])
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().hr_batch_execute(self._plan, vp, fp, _stream(self.device, stream)))
+
+    def backproject(self, volumes: list[torch.Tensor], stream=None) -> None:
+        """Only the persistent backprojection, from the filtered data of the last run."""
+        vp = (ctypes.c_void_p * len(self.scans))(*[v.data_ptr() for v in volumes])
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().hr_batch_backproject(self._plan, vp, _stream(self.device, stream)))
+
+    def select(self, variant: int) -> None:
+        _lib.check(_lib.load().hr_batch_select(self._plan, variant))
+
+    def check(self) -> None:
+        _lib.check(_lib.load().hr_batch_check(self._plan))
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(768)
+        _lib.check(_lib.load().hr_batch_describe(self._plan, buf, 768))
+        return buf.value.decode()
+
+    @property
+    def device_bytes(self) -> int:
+        return int(_lib.load().hr_batch_device_bytes(self._plan))
+
+    def close(self) -> None:
+        if self._plan:
+            _lib.load().hr_batch_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class StagePlans:
     """The three stage plans of a scan, for per-stage use and the FP64 form."""
 
@@ -231,3 +295,13 @@ def project(scan: Scan, objects: np.ndarray, out: torch.Tensor | None = None, de
                                                  a["h"], obj.data_ptr(), obj.shape[0], st.cuda_stream))
     st.synchronize()
     return out
+
+
+def add_poisson_noise(proj: torch.Tensor, I0: float, seed: int) -> torch.Tensor:
+    """In place: line integrals -> -log(max(N, 1)/I0), N ~ Poisson(I0 exp(-p)) (GPU)."""
+    if not (proj.is_cuda and proj.dtype == torch.float32 and proj.is_contiguous()):
+        raise TypeError("proj must be a contiguous CUDA float32 tensor")
+    st = torch.cuda.current_stream(proj.device)
+    _lib.check(_lib.load().hr_add_poisson_noise(proj.data_ptr(), proj.numel(), float(I0), int(seed) & ((1 << 64) - 1),
+                                                st.cuda_stream))
+    return proj

@@ -268,6 +268,30 @@ int hr_slab_describe(const hr_slab_plan* plan, char* buf, int len);
 size_t hr_slab_device_bytes(const hr_slab_plan* plan);
 void hr_slab_plan_destroy(hr_slab_plan* plan);
 
+/* ---- several scans of uneven size in one persistent launch --------------- */
+/* n (1..16) independent scans, each described as for hr_recon_plan_create
+ * (form HR_FORM_FAST): every scan's rebinning and tensor-core filter run one
+ * after the other through shared scratch, then ONE persistent backprojection
+ * launch covers all scans' (z block, column tile) work items. The sequence is
+ * captured into a CUDA graph per set of buffer addresses and replayed. At
+ * creation each scan's slices per thread are autotuned, then the batch kernel
+ * variant on the whole batch (HELIXRECON_BATCH_VARIANT pins the latter). */
+typedef struct hr_batch_plan hr_batch_plan;
+int hr_batch_plan_create(hr_batch_plan** plan, const hr_recon_desc* descs, int n);
+/* d_vols[i]: device [YN][XN][ZN] of scan i; d_fans[i]: device [ViewN][YL][ZL]. */
+int hr_batch_execute(hr_batch_plan* plan, float* const* d_vols, const float* const* d_fans, void* stream);
+/* Only the persistent backprojection launch, from the filtered data the last
+ * hr_batch_execute left in the plan (not captured; for timing the kernel). */
+int hr_batch_backproject(hr_batch_plan* plan, float* const* d_vols, void* stream);
+/* Selects a batch backprojection variant (0..2: registers unconstrained, or
+ * limited for 10 or 12 CTAs per SM); each scan keeps the slices per thread its
+ * own autotuner chose. */
+int hr_batch_select(hr_batch_plan* plan, int variant);
+int hr_batch_describe(const hr_batch_plan* plan, char* buf, int len);
+int hr_batch_check(const hr_batch_plan* plan);
+size_t hr_batch_device_bytes(const hr_batch_plan* plan);
+void hr_batch_plan_destroy(hr_batch_plan* plan);
+
 /* ---- analytic phantom projector (synthetic data source) ----------------- */
 /* Objects: nobj rows of 17 doubles [type, cx, cy, cz, a, b, c, R(9, row-major,
  * columns = body axes), mu]; type 0 ellipsoid, type 1 elliptic cylinder (z in
@@ -278,6 +302,42 @@ void hr_slab_plan_destroy(hr_slab_plan* plan);
 int hr_project_ellipsoids(float* d_proj, int YL, int ZL, int ViewN, double SO, double SD, double dYA, double YLC0,
                           double dZL, double ZLC0, double BetaS, double dBeta, double h, const double* d_obj,
                           int nobj, void* stream);
+
+/* Photon noise of a transmission scan, in place: p -> -log(max(N, 1) / I0)
+ * with N ~ Poisson(I0 exp(-p)) per sample (counter-based generator seeded by
+ * `seed`; the result does not depend on the launch). */
+int hr_add_poisson_noise(float* d_proj, long long n, double I0, unsigned long long seed, void* stream);
+
+/* ---- learned artifact correction (2.5D residual CNN) -------------------- */
+/* Corrects a half-view reconstruction toward the full-view one. Input: 5
+ * adjacent slices (u = mu/mu_w - 1, NHWC BF16, channels padded to 16); 8 conv
+ * layers 3x3 (16->32, 6 x 32->32 with ReLU, 32->16 of which channel 0 is the
+ * residual); output = centre slice + mu_w * residual. Forward and backward
+ * data passes run on the tensor cores (BF16 operands, FP32 accumulation),
+ * weight gradients on the CUDA cores; Adam on FP32 master parameters.
+ * Parameters: per layer W[co][tap][ci] (tap = 3*ky + kx) then b[co]. */
+typedef struct hr_cnn hr_cnn;
+size_t hr_cnn_param_count(void);
+int hr_cnn_create(hr_cnn** net, const float* h_params);
+int hr_cnn_get_params(const hr_cnn* net, float* h_params);
+/* Gradients of the last hr_cnn_train_step. */
+int hr_cnn_get_grads(const hr_cnn* net, float* h_grads);
+/* Forward, loss = mean(((pred - target)/mu_w)^2) and parameter gradients; lr > 0
+ * then applies one Adam step. d_x [B][H][W][16] BF16 (16-byte aligned),
+ * d_base / d_target FP32 [B][H][W]; *loss_out (if not NULL) after a sync. */
+int hr_cnn_train_step(hr_cnn* net, const uint16_t* d_x, const float* d_base, const float* d_target, int B, int H,
+                      int W, float mu_w, float lr, float* loss_out, void* stream);
+/* Inference: d_out[b*sb + (y*W+x)*sp] = base[same] + mu_w * residual. */
+int hr_cnn_forward(hr_cnn* net, float* d_out, const uint16_t* d_x, const float* d_base, long long sb, long long sp,
+                   int B, int H, int W, float mu_w, void* stream);
+/* Corrects every slice of a volume [YN][XN][ZN] (z fastest), chunk slices per pass. */
+int hr_cnn_apply_volume(hr_cnn* net, float* d_out, const float* d_vol, int XN, int YN, int ZN, float mu_w, int chunk,
+                        void* stream);
+/* Network input of slices [z0, z0+nz) of a volume (neighbours clamped at the ends). */
+int hr_cnn_pack_input(uint16_t* d_x, const float* d_vol, int XN, int YN, int ZN, int z0, int nz, float mu_w,
+                      void* stream);
+int hr_cnn_check(const hr_cnn* net);
+void hr_cnn_destroy(hr_cnn* net);
 
 #ifdef __cplusplus
 }

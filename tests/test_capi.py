@@ -58,6 +58,13 @@ def test_argument_validation_precedes_device_use():
     assert st == 1 and b"non-zero" in lib.hr_last_error()
     st = lib.hr_rebin_host(None, None, 4, 4, 4, 1.0, 0.01, 0.1, 1.0, 1.0, 0.1, 541.0)
     assert st == 1
+    descs = (_lib.ReconDesc * 17)()
+    st = lib.hr_batch_plan_create(ctypes.byref(plan), descs, 17)
+    assert st == 1 and b"1..16" in lib.hr_last_error()
+    st = lib.hr_batch_plan_create(ctypes.byref(plan), descs, 2)
+    assert st == 1 and b"weight table" in lib.hr_last_error()
+    st = lib.hr_add_poisson_noise(None, 10, 1e5, 1, None)
+    assert st == 1
 
 
 def test_no_device_is_reported_not_crashed():

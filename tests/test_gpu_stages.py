@@ -113,12 +113,13 @@ def test_bp_high_level_entry_both_branches(cuda):
 
 
 def test_scan_geom_mex_mirror(cuda):
-    sc = G.tiny(delta=8)
+    sc = G.tiny(delta=8, XN=12, YN=10, ZN=12, dx=0.5, dy=0.6, dz=0.5)
     g = sc.bp_geom()
     rng = np.random.default_rng(9)
     fp = rng.standard_normal((g["PN"], g["ZL"], g["YL"]))
     ObjR = sc.dx * sc.XN / 2
-    sc2 = G.tiny(delta=8, dx=ObjR * 2 / sc.XN, dy=ObjR * 2 / sc.YN, dz=ObjR * 2 / sc.ZN)
+    sc2 = G.tiny(delta=8, XN=sc.XN, YN=sc.YN, ZN=sc.ZN, dx=ObjR * 2 / sc.XN, dy=ObjR * 2 / sc.YN,
+                 dz=ObjR * 2 / sc.ZN)
     g2 = sc2.bp_geom()
     scan_geom = {"ScDet": [sc.SO, sc.DO, sc.YL, sc.ZL, sc.DecWidth, sc.DecHeigh, 0.0, sc.ZLC1, sc.h_norm],
                  "Proj": [g["BetaS"], 0.0, g["PN"], sc.N_2pi],
@@ -128,6 +129,7 @@ def test_scan_geom_mex_mirror(cuda):
     api.Parallel_FDK_Helical_3DWeighting(scan_geom, fp, ct, 0)
     w = oracle.weight_table(sc.N_2pi, sc.HSCoef, sc.delta)
     ref = oracle.bp_f64(fp, w, g2)
+    assert np.count_nonzero(ref) > ref.size // 2
     np.testing.assert_allclose(ct, ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
 
 

@@ -166,7 +166,8 @@ def test_filter_shim_matches_c_abi(mex, cuda):
 def test_backprojection_shim_writes_ctimage_in_place(mex, cuda, use_gpu):
     from analyticalreconbigpatient_b200 import api, geometry as G
 
-    sc = G.tiny(delta=8)
+    # the MEX derives cubic voxels dx = dy = dz = 2 ObjR / N: a 6 mm cube of 0.5 mm voxels inside the helix
+    sc = G.tiny(delta=8, XN=12, YN=12, ZN=12, dx=0.5, dy=0.5, dz=0.5)
     ObjR = sc.dx * sc.XN / 2
     g = sc.bp_geom()
     centre = [g["XNC"] + 1, g["YNC"] + 1, g["ZNC"] + 1]
