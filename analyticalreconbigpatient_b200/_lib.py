@@ -46,6 +46,18 @@ class ReconDesc(ctypes.Structure):
                 + [("bp", BpGeom), ("w", _p), ("form", _i)])
 
 
+class GeHeader(ctypes.Structure):
+    _fields_ = ([("raw", _f * 18)] + [(n, _d) for n in ("Source2DetDis", "Source2IsoDis", "DetCellPitch",
+                                                         "BeginViewAngle")]
+                + [(n, _i) for n in ("NumberOfViewPerRotation", "TotalViewNumber", "NumberOfDetChannelPerRow",
+                                     "NumberOfDetectorRow")]
+                + [(n, _d) for n in ("IsoChannelLocation", "SliceHeigh", "HelicalPitch")])
+
+
+class GeOptions(ctypes.Structure):
+    _fields_ = [("k1", _d), ("delta", _i), ("HSCoef", _d)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "hr_last_error": (ctypes.c_char_p, []),
@@ -109,6 +121,16 @@ _SIGS = {
     "hr_cnn_pack_input": (_i, [_p, _p, _i, _i, _i, _i, _i, _f, _p]),
     "hr_cnn_check": (_i, [_p]),
     "hr_cnn_destroy": (None, [_p]),
+    "hr_ge_parse_header": (_i, [_p, ctypes.POINTER(GeHeader)]),
+    "hr_ge_read_header": (_i, [ctypes.c_char_p, ctypes.POINTER(GeHeader)]),
+    "hr_ge_segments": (_i, [ctypes.POINTER(GeHeader), _i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "hr_ge_segment_views": (_i, [ctypes.POINTER(GeHeader), _i, _i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "hr_ge_read_segment": (_i, [ctypes.c_char_p, ctypes.POINTER(GeHeader), _i, _i, _p, ctypes.POINTER(_i)]),
+    "hr_ge_segment_desc": (_i, [ctypes.POINTER(GeHeader), _i, _i, _d, _i, _i, _i, ctypes.POINTER(GeOptions), _i,
+                                ctypes.POINTER(ReconDesc), _p]),
+    "hr_ge_reconstruct": (_i, [ctypes.c_char_p, ctypes.c_char_p, _i, _d, _i, _i, _i, ctypes.POINTER(GeOptions), _i,
+                               _p]),
+    "hr_accumulate": (_i, [_p, _p, ctypes.c_longlong, _p]),
     "hr_recon_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc)]),
     "hr_recon_execute": (_i, [_p, _p, _p, _p]),
     "hr_recon_execute_host": (_i, [_p, _p, _p]),

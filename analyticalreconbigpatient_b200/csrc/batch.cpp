@@ -26,6 +26,7 @@ struct hr_batch_plan {
   std::vector<uint32_t*> pairs;  // per scan: [PN][ZL][YL] BF16 channel pairs
   std::vector<int> nz;           // per scan: slices per thread of its backprojection
   float* d_rebinned = nullptr;   // shared: the largest scan's [ViewN][YL][ZL]
+  int* d_counter = nullptr;      // work-item counter of the persistent launch
   void* d_split[3] = {};         // shared tensor-core filter operands
   int variant = 0, tuned = 0;
   int ctas[hr::kBatchVariants_n] = {};
@@ -47,6 +48,7 @@ void destroy(hr_batch_plan* p) {
   for (auto* b : p->bp) hr_bp_plan_destroy(b);
   for (auto* q : p->pairs) cudaFree(q);
   cudaFree(p->d_rebinned);
+  cudaFree(p->d_counter);
   for (void* q : p->d_split) cudaFree(q);
   if (p->sc) cudaStreamDestroy(p->sc);
   delete p;
@@ -78,7 +80,7 @@ int enqueue(const hr_batch_plan* p, float* const* vols, const float* const* fans
   std::vector<hr::BpFastBatchScan> sc;
   HR_TRY(scans_of(p, vols, &sc));
   const long long items = hr::bp_fast_batch_items(sc.data(), p->n);
-  return hr::bp_fast_batch_execute(sc.data(), p->n, p->variant, 0, (int)items, p->ctas[p->variant], s);
+  return hr::bp_fast_batch_execute(sc.data(), p->n, p->variant, 0, (int)items, p->ctas[p->variant], p->d_counter, s);
 }
 
 // Picks each scan's slices per thread with its own plan's autotuner (the
@@ -131,7 +133,7 @@ int autotune(hr_batch_plan* p) {
     float ms = 1e30f;
     for (int rep = 0; rep < 2 && st == HR_OK; ++rep) {
       cudaEventRecord(e0, p->sc);
-      st = hr::bp_fast_batch_execute(sc.data(), p->n, v, 0, (int)items, p->ctas[v], p->sc);
+      st = hr::bp_fast_batch_execute(sc.data(), p->n, v, 0, (int)items, p->ctas[v], p->d_counter, p->sc);
       cudaEventRecord(e1, p->sc);
       if (cudaEventSynchronize(e1) != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "batch autotune: launch failed");
       float t = 0.f;
@@ -179,6 +181,7 @@ extern "C" int hr_batch_plan_create(hr_batch_plan** plan, const hr_recon_desc* d
     split_max = std::max(split_max, hr::filter_tc_scratch_bytes(descs[i].YL, descs[i].ZL, descs[i].bp.PN));
   }
   int st = alloc(p, (void**)&p->d_rebinned, nfan_max * sizeof(float));
+  if (st == HR_OK) st = alloc(p, (void**)&p->d_counter, sizeof(int));
   for (int k = 0; k < 3 && st == HR_OK; ++k) st = alloc(p, &p->d_split[k], split_max);
   for (int i = 0; i < n && st == HR_OK; ++i) {
     const hr_recon_desc& d = descs[i];
@@ -250,7 +253,7 @@ extern "C" int hr_batch_backproject(hr_batch_plan* p, float* const* d_vols, void
   std::vector<hr::BpFastBatchScan> sc;
   HR_TRY(scans_of(p, d_vols, &sc));
   const long long items = hr::bp_fast_batch_items(sc.data(), p->n);
-  return hr::bp_fast_batch_execute(sc.data(), p->n, p->variant, 0, (int)items, p->ctas[p->variant],
+  return hr::bp_fast_batch_execute(sc.data(), p->n, p->variant, 0, (int)items, p->ctas[p->variant], p->d_counter,
                                    hr::as_stream(stream));
 }
 

@@ -321,10 +321,12 @@ __global__ void __launch_bounds__(kBx* kBy) bp_fast_kernel(float* __restrict__ v
 
 // Several scans of uneven size in one persistent launch. Work items are
 // (scan, z block, column tile), numbered scan by scan with the column tile
-// fastest, and dealt to the resident CTAs round robin (items that run
-// together share a z block and so its views in L2). Each scan keeps the
-// slices per thread its own geometry favours (16, 8 or 4: a uniform branch
-// per item).
+// fastest; each CTA claims the next item from a global counter when it
+// finishes one, so the items in flight stay a narrow window of the order (a
+// few z blocks, whose views stay in L2), as under the hardware block
+// scheduler; a static round robin lets CTAs drift apart and spreads the
+// window over many z blocks. Each scan keeps the slices per thread its own
+// geometry favours (16, 8 or 4: a uniform branch per item).
 struct BatchScan {
   FastParams P;
   ZTabs T;
@@ -337,12 +339,20 @@ struct BatchParams {
   int n;
   int begin, count;  // items [begin, begin + count)
   int grid;          // CTAs launched
+  int* counter;      // zero at launch
 };
 
 // MB: CTAs per SM the register allocation must allow (1: no constraint).
 template <int MB>
 __global__ void __launch_bounds__(kBx* kBy, MB) bp_fast_batch_kernel(const __grid_constant__ BatchParams B) {
-  for (int k = blockIdx.x; k < B.count; k += gridDim.x) {
+  __shared__ int s_item;
+  const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
+  for (;;) {
+    if (leader) s_item = atomicAdd(B.counter, 1);
+    __syncthreads();
+    const int k = s_item;
+    __syncthreads();
+    if (k >= B.count) break;
     const int item = B.begin + k;
     int sc = 0;
     while (sc + 1 < B.n && item >= B.s[sc + 1].item0) ++sc;
@@ -618,8 +628,9 @@ static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t 
 int bp_fast_batch_grid(int bv, int* ctas) { return batch_dispatch(bv, nullptr, ctas, nullptr); }
 
 int bp_fast_batch_execute(const BpFastBatchScan* scans, int n, int bv, int begin, int count, int ctas,
-                          cudaStream_t s) {
+                          int* d_counter, cudaStream_t s) {
   HR_REQUIRE(n >= 1 && n <= kBatchMaxScans, "batch backprojection: %d scans (1..%d per launch)", n, kBatchMaxScans);
+  HR_REQUIRE(d_counter != nullptr, "batch backprojection: no work counter");
   HR_REQUIRE(bv >= 0 && bv < kBatchVariants_n, "batch backprojection: unknown variant %d", bv);
   HR_REQUIRE(ctas >= 1, "batch backprojection: no CTAs");
   BatchParams B{};
@@ -647,7 +658,9 @@ int bp_fast_batch_execute(const BpFastBatchScan* scans, int n, int bv, int begin
   B.begin = begin;
   B.count = count;
   B.grid = std::min(ctas, std::max(count, 1));
+  B.counter = d_counter;
   if (count == 0) return HR_OK;
+  HR_CUDA_TRY(cudaMemsetAsync(d_counter, 0, sizeof(int), s));
   return batch_dispatch(bv, &B, nullptr, s);
 }
 

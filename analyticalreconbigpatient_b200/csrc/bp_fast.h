@@ -101,9 +101,10 @@ struct BpFastBatchScan {
 long long bp_fast_batch_items(const BpFastBatchScan* scans, int n);
 // Persistent CTAs a launch of batch variant bv keeps resident (occupancy x SMs).
 int bp_fast_batch_grid(int bv, int* ctas);
-// Backprojects items [begin, begin + count) of the batch with at most ctas CTAs.
+// Backprojects items [begin, begin + count) of the batch with at most ctas CTAs;
+// d_counter: a device int the launch consumes (zeroed on the stream first).
 int bp_fast_batch_execute(const BpFastBatchScan* scans, int n, int bv, int begin, int count, int ctas,
-                          cudaStream_t s);
+                          int* d_counter, cudaStream_t s);
 // Slices per thread of the fastest per-slice variant the plan's autotuner timed (8 if untuned).
 int bp_fast_best_per_slice_nz(const BpFast& f);
 // The fast-form geometry and tables of a backprojection plan (HR_FORM_FAST).

@@ -8,19 +8,25 @@
 //   output : centre slice (FP32, not rounded) + mu_w * L8 channel 0
 //
 // Convolutions run as implicit GEMMs on the 5th-generation tensor cores: one
-// CTA tile is 128 output pixels of one image row (M = 128, TMEM lanes) by COUT
-// channels (N), K = 9 taps x CIN channels. The CTA stages a 3 x 130-pixel halo
-// of the input in shared memory in the K-major no-swizzle layout (one plane of
-// 16-byte pixel chunks per 8-channel group), so the A operand of tap (dy, dx)
-// is the same buffer viewed from another 16-byte-aligned start address: every
-// input pixel is loaded once per tile, and nine descriptor offsets replace an
-// im2col copy. The weights (B operand) stay in shared memory for the CTA's
-// life; one thread issues the 9*CIN/16 tcgen05.mma of a tile and commits to
-// an mbarrier (bounded wait); all four warps then read their 32 TMEM lanes
-// and run the epilogue (bias + ReLU + BF16 store; gradient masking by the
-// forward activation; fused residual + loss + output gradient). The backward
-// data pass is the same kernel with the weights transposed and flipped. Weight
-// gradients are a register-tiled FP32 reduction on the CUDA cores.
+// tile is 128 output pixels of one image row (M = 128, TMEM lanes) by COUT
+// channels (N), K = 9 taps x CIN channels. A 3 x 130-pixel halo of the input
+// is staged in shared memory in the K-major no-swizzle layout (one plane of
+// 16-byte pixel chunks per 8-channel group; each plane is one TMA box of 8
+// channels x 130 pixels, zero-filled outside the image), so the A operand of
+// tap (dy, dx) is the same buffer seen from another 16-byte-aligned start
+// address: every input pixel is loaded once per tile and nine descriptor
+// offsets replace an im2col copy. The weights (B operand) stay in shared
+// memory for the CTA's life. Persistent, warp-specialised CTAs: warp 0 issues
+// the TMA loads into a 3-stage halo ring, warp 1 issues the 9*CIN/16
+// tcgen05.mma of a tile into one of two TMEM accumulators, warps 2-5 read the
+// other accumulator and run the epilogue (bias + ReLU + BF16 store; gradient
+// masking by the forward activation; fused residual + loss + output
+// gradient), so loads, MMAs and stores of consecutive tiles overlap. Every
+// mbarrier wait is bounded and sets an error flag when it gives up. The
+// backward data pass is the same kernel with the weights transposed and
+// flipped. Weight gradients are a register-tiled FP32 reduction on the CUDA
+// cores.
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -34,8 +40,11 @@ namespace {
 
 constexpr int kTileM = 128;                  // output pixels per tile (one row segment)
 constexpr int kHalo = kTileM + 2;            // halo pixels per row
-constexpr int kPlane = kHalo * 16;           // bytes of one 8-channel plane of a halo row
-constexpr int kThreads = 128;
+constexpr int kBox = kHalo * 16;             // bytes of one TMA box: 8 channels x 130 pixels
+constexpr int kPlane = 17 * 128;             // plane stride: one box, 128-byte aligned
+constexpr int kStages = 3;                   // halo ring
+constexpr int kThreads = 192;                // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int kTmemCols = 64;                // two 32-column accumulators
 constexpr uint32_t kWaitLimit = 1u << 22;    // try_wait rounds before a wait is declared hung
 constexpr int kLayers = 8;
 constexpr int kCin[kLayers] = {16, 32, 32, 32, 32, 32, 32, 32};
@@ -69,7 +78,10 @@ __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, ui
       : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+// Bounded wait on an mbarrier phase; gives up (returning false) when another
+// role of the CTA has aborted, or after kWaitLimit rounds (then records the
+// error and aborts the CTA).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatile int* abort_flag, int* err) {
   const uint32_t addr = smem_u32(bar);
   for (uint32_t i = 0; i < kWaitLimit; ++i) {
     uint32_t done;
@@ -81,8 +93,39 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
         : "r"(addr), "r"(phase)
         : "memory");
     if (done) return true;
+    if (*abort_flag) return false;
   }
+  atomicExch(err, 1);
+  *abort_flag = 1;
   return false;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// 4D tiled TMA load (no multicast): box {8 channels, 130 pixels, 1 row, 1 image}.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, uint64_t* bar, int c, int x, int y,
+                                            int b) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+      "[%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c), "r"(x), "r"(y), "r"(b)
+      : "memory");
 }
 
 __device__ __forceinline__ float bf_lo(uint32_t w) { return __uint_as_float(w << 16); }
@@ -122,6 +165,7 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float (&v)[32]) {
 }
 
 struct ConvArgs {
+  CUtensorMap in_map;    // the input as a 4D tensor {CIN, W, H, B} of BF16, box {8, 130, 1, 1}
   const uint16_t* in;    // NHWC BF16 [B][H][W][CIN]
   const uint16_t* wimg;  // B operand image [9*CIN/8][COUT][8] BF16
   const float* bias;     // [COUT] (EPI_RELU, EPI_LOSS, EPI_RESID)
@@ -141,143 +185,169 @@ struct ConvArgs {
 
 template <int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant__ ConvArgs a) {
-  constexpr int G = CIN / 8;                 // 16-byte chunks per input pixel
+  constexpr int G = CIN / 8;                 // 8-channel groups (TMA boxes per halo row)
   constexpr int kRow = G * kPlane;           // bytes of one halo row
+  constexpr int kStageBytes = 3 * kRow;
   constexpr int kWBytes = 9 * CIN * COUT * 2;
   constexpr int kKSteps = 9 * CIN / 16;
   constexpr uint32_t kIdesc = idesc_bf16(COUT);
+  constexpr uint32_t kTxBytes = 3 * G * kBox;
   static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "unsupported channel counts");
-  extern __shared__ __align__(128) uint8_t smem[];
-  uint8_t* halo = smem;                      // 3 rows
-  uint8_t* wsm = smem + 3 * kRow;            // weights
-  uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + kWBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
-  int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint8_t* wsm = smem + kStages * kStageBytes;  // weights
+  uint64_t* full = reinterpret_cast<uint64_t*>(wsm + kWBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* tfull = empty + kStages;
+  uint64_t* tempty = tfull + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // weights: a straight copy of the prepared image
   for (int i = tid; i < kWBytes / 16; i += kThreads)
     reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.wimg) + i);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&tfull[s], 1);
+      mbar_init(&tempty[s], 128);
+    }
     *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(tmem_slot)));
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const uint32_t halo_a = smem_u32(halo), w_a = smem_u32(wsm);
+  const uint32_t smem_a = smem_u32(smem), w_a = smem_u32(wsm);
 
   const int nseg = (a.W + kTileM - 1) / kTileM;
   const long long tiles = (long long)a.B * a.H * nseg;
-  uint32_t phase = 0;
-  for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const int seg = (int)(t % nseg);
-    const long long by = t / nseg;
-    const int y = (int)(by % a.H), b = (int)(by / a.H);
-    const int x0 = seg * kTileM;
-    // ---- halo: rows y-1..y+1, pixels x0-1..x0+128, zero outside the image
-    for (int i = tid; i < 3 * kHalo * G; i += kThreads) {
-      const int r = i / (kHalo * G), rem = i - r * (kHalo * G);
-      const int pix = rem / G, g = rem - pix * G;
-      const int yy = y + r - 1, xx = x0 + pix - 1;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (yy >= 0 && yy < a.H && xx >= 0 && xx < a.W)
-        v = __ldg(reinterpret_cast<const uint4*>(a.in + (((size_t)b * a.H + yy) * a.W + xx) * CIN) + g);
-      *reinterpret_cast<uint4*>(halo + r * kRow + g * kPlane + pix * 16) = v;
+  if (warp == 0) {
+    // ---- producer: the halo of each tile, 3 rows x G boxes --------------------------------
+    if (lane == 0) {
+      int it = 0;
+      for (long long t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+        const int s = it % kStages;
+        if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, abort_flag, a.err)) break;
+        const int seg = (int)(t % nseg);
+        const long long by = t / nseg;
+        const int y = (int)(by % a.H), b = (int)(by / a.H);
+        mbar_expect_tx(&full[s], kTxBytes);
+        const uint32_t st = smem_a + s * kStageBytes;
+        for (int r = 0; r < 3; ++r)
+          for (int g = 0; g < G; ++g)
+            tma_load_4d(st + r * kRow + g * kPlane, &a.in_map, &full[s], g * 8, seg * kTileM - 1, y + r - 1, b);
+      }
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
+  } else if (warp == 1) {
+    // ---- MMA issuer --------------------------------------------------------------------------
+    if (lane == 0) {
+      int it = 0;
+      for (long long t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+        const int s = it % kStages, acc = it & 1;
+        if (!mbar_wait(&full[s], (it / kStages) & 1, abort_flag, a.err)) break;
+        if (it >= 2 && !mbar_wait(&tempty[acc], ((it >> 1) - 1) & 1, abort_flag, a.err)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t st = smem_a + s * kStageBytes;
+#pragma unroll
+        for (int k = 0; k < kKSteps; ++k) {
+          const int k0 = k * 16;
+          const int tap = k0 / CIN, c0 = k0 - tap * CIN;
+          const int dy = tap / 3, dx = tap - dy * 3;  // halo row and pixel offset
+          const uint64_t ad = desc_noswz(st + dy * kRow + (c0 / 8) * kPlane + dx * 16, kPlane, 128);
+          const uint64_t bd = desc_noswz(w_a + (k0 / 8) * (COUT * 16), COUT * 16, 128);
+          umma(tmem + acc * 32, ad, bd, kIdesc, k > 0 ? 1u : 0u);
+        }
+        umma_commit(&empty[s]);    // the halo stage may be refilled
+        umma_commit(&tfull[acc]);  // the accumulator is ready
+      }
+    }
+  } else {
+    // ---- epilogue: warps 2-5, TMEM lane quarter warp % 4 --------------------------------------
+    const int q = warp & 3;
+    int it = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+      const int acc = it & 1;
+      if (!mbar_wait(&tfull[acc], (it >> 1) & 1, abort_flag, a.err)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-      for (int s = 0; s < kKSteps; ++s) {
-        const int k0 = s * 16;
-        const int tap = k0 / CIN, c0 = k0 - tap * CIN;
-        const int dy = tap / 3, dx = tap - dy * 3;  // 0..2: halo row and pixel offset
-        const uint64_t ad = desc_noswz(halo_a + dy * kRow + (c0 / 8) * kPlane + dx * 16, kPlane, 128);
-        const uint64_t bd = desc_noswz(w_a + (k0 / 8) * (COUT * 16), COUT * 16, 128);
-        umma(tmem, ad, bd, kIdesc, s > 0 ? 1u : 0u);
-      }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(bar))
-                   : "memory");
-    }
-    // every thread waits; the CTA leaves together if any wait gave up
-    const int ok = __syncthreads_and(mbar_wait(bar, phase) ? 1 : 0);
-    phase ^= 1u;
-    if (!ok) {
-      if (tid == 0) atomicExch(a.err, 1);
-      break;
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    float acc[COUT];
-    tmem_ld<COUT>(tmem + ((uint32_t)(warp * 32) << 16), acc);
-    const int x = x0 + warp * 32 + lane;
-    const bool valid = x < a.W;
-    const size_t pix = ((size_t)b * a.H + y) * a.W + x;
-    if constexpr (EPI == EPI_RELU) {
-      if (valid) {
-        uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
-#pragma unroll
-        for (int q = 0; q < COUT / 8; ++q) {
-          float v[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) v[j] = fmaxf(acc[8 * q + j] + __ldg(a.bias + 8 * q + j), 0.0f);
-          o[q] = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
-        }
-      }
-    } else if constexpr (EPI == EPI_MASK) {
-      if (valid) {
-        const uint4* m = reinterpret_cast<const uint4*>(a.mask + pix * COUT);
-        uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
-#pragma unroll
-        for (int q = 0; q < COUT / 8; ++q) {
-          const uint4 mv = __ldg(m + q);
-          const uint32_t mw[4] = {mv.x, mv.y, mv.z, mv.w};
-          float v[8];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            v[2 * j] = bf_lo(mw[j]) > 0.0f ? acc[8 * q + 2 * j] : 0.0f;
-            v[2 * j + 1] = bf_hi(mw[j]) > 0.0f ? acc[8 * q + 2 * j + 1] : 0.0f;
-          }
-          o[q] = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
-        }
-      }
-    } else {
-      const float r = acc[0] + __ldg(a.bias);
-      float e2 = 0.0f;
-      if (valid) {
-        const size_t off = (size_t)b * a.sb + ((size_t)y * a.W + x) * a.sp;
-        const float p = a.base[off] + a.scale * r;
-        if constexpr (EPI == EPI_RESID) {
-          a.pred[off] = p;
-        } else {
-          if (a.pred) a.pred[off] = p;
-          const float e = (p - a.target[off]) / a.scale;
-          e2 = e * e;
+      float v[COUT];
+      tmem_ld<COUT>(tmem + acc * 32 + ((uint32_t)(q * 32) << 16), v);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&tempty[acc]);  // the registers hold the tile: the accumulator may be reused
+      const int seg = (int)(t % nseg);
+      const long long by = t / nseg;
+      const int y = (int)(by % a.H), b = (int)(by / a.H);
+      const int x = seg * kTileM + q * 32 + lane;
+      const bool valid = x < a.W;
+      const size_t pix = ((size_t)b * a.H + y) * a.W + x;
+      if constexpr (EPI == EPI_RELU) {
+        if (valid) {
           uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
-          o[0] = make_uint4(pack2(a.grad_scale * e, 0.0f), 0u, 0u, 0u);
 #pragma unroll
-          for (int q = 1; q < COUT / 8; ++q) o[q] = make_uint4(0u, 0u, 0u, 0u);
+          for (int c = 0; c < COUT / 8; ++c) {
+            float u[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) u[j] = fmaxf(v[8 * c + j] + __ldg(a.bias + 8 * c + j), 0.0f);
+            o[c] = make_uint4(pack2(u[0], u[1]), pack2(u[2], u[3]), pack2(u[4], u[5]), pack2(u[6], u[7]));
+          }
+        }
+      } else if constexpr (EPI == EPI_MASK) {
+        if (valid) {
+          const uint4* m = reinterpret_cast<const uint4*>(a.mask + pix * COUT);
+          uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
+#pragma unroll
+          for (int c = 0; c < COUT / 8; ++c) {
+            const uint4 mv = __ldg(m + c);
+            const uint32_t mw[4] = {mv.x, mv.y, mv.z, mv.w};
+            float u[8];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              u[2 * j] = bf_lo(mw[j]) > 0.0f ? v[8 * c + 2 * j] : 0.0f;
+              u[2 * j + 1] = bf_hi(mw[j]) > 0.0f ? v[8 * c + 2 * j + 1] : 0.0f;
+            }
+            o[c] = make_uint4(pack2(u[0], u[1]), pack2(u[2], u[3]), pack2(u[4], u[5]), pack2(u[6], u[7]));
+          }
+        }
+      } else {
+        const float r = v[0] + __ldg(a.bias);
+        float e2 = 0.0f;
+        if (valid) {
+          const size_t off = (size_t)b * a.sb + ((size_t)y * a.W + x) * a.sp;
+          const float pr = a.base[off] + a.scale * r;
+          if constexpr (EPI == EPI_RESID) {
+            a.pred[off] = pr;
+          } else {
+            if (a.pred) a.pred[off] = pr;
+            const float e = (pr - a.target[off]) / a.scale;
+            e2 = e * e;
+            uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
+            o[0] = make_uint4(pack2(a.grad_scale * e, 0.0f), 0u, 0u, 0u);
+#pragma unroll
+            for (int c = 1; c < COUT / 8; ++c) o[c] = make_uint4(0u, 0u, 0u, 0u);
+          }
+        }
+        if constexpr (EPI == EPI_LOSS) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+          if (lane == 0 && e2 != 0.0f) atomicAdd(a.loss, e2);
         }
       }
-      if constexpr (EPI == EPI_LOSS) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
-        if (lane == 0 && e2 != 0.0f) atomicAdd(a.loss, e2);
-      }
     }
-    // all TMEM reads of this tile are done before the next tile's MMAs overwrite it
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
   }
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem));
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  }
 }
 
 // Weight gradients on the CUDA cores: dW[co][tap][ci] += sum_p G[p][co] X[p + tap][ci],
@@ -410,19 +480,51 @@ __global__ void pack_input_kernel(uint16_t* __restrict__ out, const float* __res
   }
 }
 
-// Dynamic shared memory of a conv CTA: halo + weights + barrier, padded so
-// that every address an operand descriptor of the kernel can reach lies inside
-// the allocation (start of the last tap's A operand + 16 eight-row groups).
-template <int CIN, int COUT, int EPI>
-size_t conv_smem() {
-  const size_t used = (size_t)3 * (CIN / 8) * kPlane + 9 * CIN * COUT * 2 + 64;
-  const size_t reach = (size_t)2 * (CIN / 8) * kPlane + (CIN / 8 - 1) * kPlane + 32 + 16 * (size_t)kPlane + 256;
-  return std::max(used, reach);
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int get_encoder(EncodeTiledFn* fn) {
+  static EncodeTiledFn cached = nullptr;
+  if (!cached) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    HR_CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || p == nullptr)
+      return hr::fail(HR_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available");
+    cached = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  *fn = cached;
+  return HR_OK;
+}
+
+// The NHWC BF16 activation [B][H][W][C] as a 4D TMA tensor {C, W, H, B}; box
+// {8, 130, 1, 1}; out-of-range elements read as zero (the conv padding).
+int make_act_map(CUtensorMap* map, const void* base, int C, int B, int H, int W) {
+  EncodeTiledFn enc;
+  HR_TRY(get_encoder(&enc));
+  HR_REQUIRE(((uintptr_t)base & 15) == 0, "conv: activation must be 16-byte aligned");
+  const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+  const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+  const cuuint32_t box[4] = {8, (cuuint32_t)kHalo, 1, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return hr::fail(HR_ERR_CUDA, "cuTensorMapEncodeTiled (activation) failed (%d)", (int)r);
+  return HR_OK;
+}
+
+// Dynamic shared memory of a conv CTA: halo ring + weights + barriers + alignment slack.
+template <int CIN, int COUT>
+constexpr size_t conv_smem() {
+  return (size_t)kStages * 3 * (CIN / 8) * kPlane + 9 * CIN * COUT * 2 + 256 + 128;
 }
 
 template <int CIN, int COUT, int EPI>
-int launch_conv(const ConvArgs& a, cudaStream_t s) {
-  const size_t smem = conv_smem<CIN, COUT, EPI>();
+int launch_conv(ConvArgs& a, cudaStream_t s) {
+  const size_t smem = conv_smem<CIN, COUT>();
+  HR_TRY(make_act_map(&a.in_map, a.in, CIN, a.B, a.H, a.W));
   HR_CUDA_TRY(cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
   int per_sm = 0;

@@ -49,7 +49,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["full", "medium", "small", "bigpatient", "batch"], default="full")
+    ap.add_argument("--config", choices=["full", "medium", "small", "bigpatient", "batch", "learned"], default="full")
+    ap.add_argument("--train-phantoms", type=int, default=2000, help="learned: training phantoms")
+    ap.add_argument("--train-steps", type=int, default=2000, help="learned: Adam steps (batch 8)")
+    ap.add_argument("--eval-phantoms", type=int, default=100, help="learned: held-out phantoms")
     ap.add_argument("--slab", type=int, default=64, help="slices per slab (bigpatient)")
     ap.add_argument("--form", choices=["fast", "plain"], default="fast",
                     help="form timed as `value` (the chosen BF16 form by default); the plain FP32 form is "
@@ -538,6 +541,128 @@ def run_batch(args, dev, world, rank, barrier):
         print(json.dumps(line), flush=True)
 
 
+def run_learned(args, dev, world, rank, barrier):
+    """Half-view (492 views/rot) plain reconstruction corrected by the 2.5D CNN,
+    trained on pairs the plain method makes from seeded noisy phantoms, against
+    the full-view (984 views/rot) plain reconstruction: HU RMSE on held-out
+    phantoms, and seconds per 10-rotation volume end to end."""
+    import torch
+    import torch.distributed as dist
+
+    from analyticalreconbigpatient_b200 import _lib, geometry as G, learned as L, phantom as P
+    from analyticalreconbigpatient_b200.pipeline import HelicalRecon, add_poisson_noise, project
+
+    t_start = time.perf_counter()
+    train = L.PairSet(range(1, 1 + args.train_phantoms), device=dev.index)
+    t_data = time.perf_counter() - t_start
+    net = L.Corrector(seed=rank, device=dev)
+    t0 = time.perf_counter()
+    losses = L.train(net, train, steps=args.train_steps, batch=8, lr=1e-3, seed=rank)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    del train
+    torch.cuda.empty_cache()
+    test = L.PairSet(range(100001, 100001 + args.eval_phantoms), device=dev.index)
+    ev = L.evaluate(net, test)
+    del test
+    torch.cuda.empty_cache()
+
+    # ---- one 10-rotation volume: full-view plain vs half-view plain + CNN ---------
+    full = G.Scan(ZL=64, pitch=0.984, rotations=10, N_2pi=984, XN=512, YN=512, ZN=1, dx=0.9766, dy=0.9766,
+                  dz=0.625)
+    full = G.replace(full, beta_start=full.BetaS)
+    half = G.replace(full, N_2pi=492).with_full_z()
+    full = G.replace(full, ZN=half.ZN)
+    zlo = full.h * full.BetaS / (2 * np.pi)
+    zhi = full.h * (full.BetaS + full.views * full.dBeta) / (2 * np.pi)
+    fan = project(full, P.random_ellipsoids(200001 + rank, 60, (zlo, zhi)), device=dev.index)
+    add_poisson_noise(fan, 1e5, 0x5EED0000 + 200001 + rank)
+    h_full = torch.empty(fan.shape, dtype=torch.float32, pin_memory=True)
+    h_full.copy_(fan)
+    h_half = torch.empty((half.views, half.YL, half.ZL), dtype=torch.float32, pin_memory=True)
+    h_half.copy_(fan[::2])
+    del fan
+    rf = HelicalRecon(full, form=_lib.HR_FORM_PLAIN, device=dev)
+    rh = HelicalRecon(half, form=_lib.HR_FORM_PLAIN, device=dev)
+    d_half = torch.empty(h_half.shape, dtype=torch.float32, device=dev)
+    v_half = torch.empty((half.YN, half.XN, half.ZN), dtype=torch.float32, device=dev)
+    v_out = torch.empty_like(v_half)
+    h_out = torch.empty(v_half.shape, dtype=torch.float32, pin_memory=True)
+    h_ref = torch.empty(v_half.shape, dtype=torch.float32, pin_memory=True)
+
+    def learned_step():
+        d_half.copy_(h_half, non_blocking=True)
+        rh.run(d_half, v_half)
+        net.apply_volume(v_half, v_out)
+        h_out.copy_(v_out, non_blocking=True)
+        torch.cuda.synchronize()
+
+    def full_step():
+        rf.run_host(h_full, h_ref)
+
+    for _ in range(args.warmup):
+        learned_step()
+        full_step()
+    barrier()
+    clocks = ClockSampler(None)
+    clocks.start()
+    tl, tf, tc = [], [], []
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        learned_step()
+        tl.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        full_step()
+        tf.append(time.perf_counter() - t)
+        e0.record(stream)
+        net.apply_volume(v_half, v_out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tc.append(e0.elapsed_time(e1))
+    clocks.stop()
+    s_learned, s_full = statistics.median(tl), statistics.median(tf)
+    cnn_ms = statistics.median(tc)
+    ref = h_ref.to(dev)
+    hu_learned, hu_half = L.hu_rmse(v_out, ref), L.hu_rmse(v_half, ref)
+    net.check()
+    rf.close()
+    rh.close()
+    # network FLOPs per slice: 2 * pixels * sum(9 * cin * cout) (padded channels counted)
+    flops = 2.0 * half.XN * half.YN * sum(9 * ci * co for ci, co in zip(L.CIN, L.COUT)) * half.ZN
+    pk, pk_kind = peaks()
+    tflops = flops / (cnn_ms * 1e-3) / 1e12
+    upd_half = half.updates()
+    line = {"metric": "GUPS (voxel-view updates/s, rebin+filter+3D-weighted helical BP)",
+            "value": upd_half * world / s_learned / 1e9, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": s_learned * 1e3, "s_per_volume": s_learned,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+            "data": "synthetic (seeded random-ellipsoid phantoms, Poisson noise at I0=1e5)",
+            "form": "learned (half-view plain + 2.5D CNN)",
+            "config": {"workload": f"helical 888x64, pitch 0.984, 10 rot at 492 views/rot (every second view of "
+                                   f"the 984-view scan) -> 512x512x{half.ZN} @ 0.9766x0.9766x0.625 mm",
+                       "updates_per_volume": upd_half, "flush": "inputs larger than L2 (1.1 GB of fan data)"},
+            "learned": {"train_phantoms": args.train_phantoms, "train_slices": args.train_phantoms * 16,
+                        "train_steps": args.train_steps, "batch": 8, "train_s": t_train, "data_s": t_data,
+                        "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:])),
+                        "held_out_phantoms": args.eval_phantoms, **ev,
+                        "volume_hu_rmse_learned": hu_learned, "volume_hu_rmse_half_view": hu_half,
+                        "s_per_volume_learned": s_learned, "s_per_volume_full_view_plain": s_full,
+                        "speedup_vs_full_view_plain": s_full / s_learned, "cnn_ms_per_volume": cnn_ms},
+            "roofline": {"bound": "tensor", "kernel": "conv_tc_kernel (8 layers, whole volume)", "achieved": tflops,
+                         "peak": pk["bf16_tflops"], "unit": "TFLOP/s", "frac": tflops / pk["bf16_tflops"],
+                         "peak_source": pk_kind, "traffic": None,
+                         "note": "network FLOPs (padded channels) / CNN time per volume; the conv layers are "
+                                 "bound by activation traffic (32 channels: 144 FLOP per byte)"},
+            "e2e": {"value": upd_half * world / s_learned / 1e9, "unit": "GUPS", "s_per_volume": s_learned,
+                    "h2d_bytes_per_step": half.projection_bytes(), "d2h_bytes_per_step": half.volume_bytes(),
+                    "entry": "HelicalRecon.run + Corrector.apply_volume, pinned host fan in, volume out"},
+            "gpu_launches": None, "clocks": clocks.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     import torch
@@ -549,7 +674,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    scan = G.config("full" if args.config == "batch" else args.config)
+    scan = G.config("full" if args.config in ("batch", "learned") else args.config)
     if args.impl == "reference":
         run_reference(args, scan, rank, world)
         return
@@ -564,9 +689,11 @@ def main():
         if world > 1:
             dist.barrier()
 
-    if args.config in ("bigpatient", "batch"):
+    if args.config in ("bigpatient", "batch", "learned"):
         if args.config == "batch":
             run_batch(args, dev, world, rank, barrier)
+        elif args.config == "learned":
+            run_learned(args, dev, world, rank, barrier)
         else:
             run_bigpatient(args, scan, dev, world, rank, barrier)
         if world > 1:

@@ -339,6 +339,50 @@ int hr_cnn_pack_input(uint16_t* d_x, const float* d_vol, int XN, int YN, int ZN,
 int hr_cnn_check(const hr_cnn* net);
 void hr_cnn_destroy(hr_cnn* net);
 
+/* ---- GE raw data and the segment driver ---------------------------------- */
+/* The header file of a GE scan: 18 floats (GetHeadofGeDataSet.m:20-30,
+ * 0-based: [2] source-detector, [3] source-iso, [4] cell pitch at the detector
+ * (mm), [5] first view angle (degrees), [8] views per rotation, [9] total
+ * views, [10] channels per row, [11] iso channel (1-based), [12] rows, [13]
+ * slice height at iso (mm), [14] helical pitch (table feed / slice height)).
+ * The projection file: float32 [view][row][channel], no header. */
+typedef struct hr_ge_header {
+  float raw[18];
+  double Source2DetDis, Source2IsoDis, DetCellPitch, BeginViewAngle;
+  int NumberOfViewPerRotation, TotalViewNumber, NumberOfDetChannelPerRow, NumberOfDetectorRow;
+  double IsoChannelLocation, SliceHeigh, HelicalPitch;
+} hr_ge_header;
+/* Reconstruction options of analyticalReconBigPatient.m:14-28 (NULL: k1 = 5,
+ * delta = 60, HSCoef = 0.68). */
+typedef struct hr_ge_options {
+  double k1;
+  int delta;
+  double HSCoef;
+} hr_ge_options;
+int hr_ge_parse_header(const float* raw18, hr_ge_header* h);
+int hr_ge_read_header(const char* path, hr_ge_header* h);
+/* Segment overlap (half fan in views + 1) and count (analyticalRecon.m:15-17). */
+int hr_ge_segments(const hr_ge_header* h, int seg_length, int* seg_overlap, int* seg_num);
+/* First view and view count of segment seg_ind (1-based; readBigPatientData.m:16-23). */
+int hr_ge_segment_views(const hr_ge_header* h, int seg_length, int seg_ind, int* first_view, int* dlength);
+/* Reads segment seg_ind into fan [dlength][YL][ZL] with the channels flipped
+ * (analyticalReconBigPatient.m:30), the layout the rebinning takes. fan holds
+ * seg_length*YL*ZL floats. */
+int hr_ge_read_segment(const char* path, const hr_ge_header* h, int seg_length, int seg_ind, float* fan,
+                       int* dlength);
+/* The whole-chain description of segment seg_ind (analyticalReconBigPatient.m:
+ * 31-146 with the MEX field mapping): rebinning arguments, crop, filter
+ * arguments, backprojection geometry (cubic voxels 2 objR/N, ZC = 10) and the
+ * view weights w[N_2pi] (desc->w points at w). */
+int hr_ge_segment_desc(const hr_ge_header* h, int seg_length, int seg_ind, double objR, int XN, int YN, int ZN,
+                       const hr_ge_options* opt, int form, hr_recon_desc* desc, double* w);
+/* analyticalRecon.m: every segment read, reconstructed on the GPU and summed
+ * into h_vol [YN][XN][ZN]. */
+int hr_ge_reconstruct(const char* proj_path, const char* head_path, int seg_length, double objR, int XN, int YN,
+                      int ZN, const hr_ge_options* opt, int form, float* h_vol);
+/* d_sum[i] += d_x[i] for i < n. */
+int hr_accumulate(float* d_sum, const float* d_x, long long n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
