@@ -2,20 +2,22 @@
 //
 // Same algorithm as the plain form (src/Parallel_FDK_Helical_3DWeighting.cpp:
 // 42-113, views s1..s2), rearranged so that a voxel-view update costs one FMA
-// for the detector row, two 32-bit gathers and two SFU operations:
+// for the detector row, two 32-bit gathers, one FMA and one SFU reciprocal
+// for the weight:
 //
-//   weight = w1 Gc^k1 / (w2 G^k1 + w1 Gc^k1) = 1 / (1 + 2^(Q + C))
+//   weight = w1 Gc^k1 / (w2 G^k1 + w1 Gc^k1) = 1 / (1 + 2^Q 2^C)
 //   Q(view, slice) = k1 (log2|t2| - log2|t2 -/+ 0.5|) + log2(w2/w1)
 //   C(column, view) = k1 log2((temp1 - UU)/(temp1 + UU))
 //
-// with t2 = z - h View/2pi. t2 and Q depend only on (view, slice): they are
+// with t2 = z - h View/2pi. t2 and 2^Q depend only on (view, slice): they are
 // evaluated once per plan in FP64 (the helical source position accumulates
-// over ~1e4-1e5 views) and stored per z block as a float2 table; a CTA covers
+// over ~1e4-1e5 views) and stored per z block as a float2 table (2^Q is 0 or
+// +inf where a view weight w is 0, which gives the weights 1 and 0); a CTA covers
 // one z block, so every thread of a CTA reads the same table entry (broadcast)
 // and a per-(block, view) bit mask tells which of its slices have the view in
 // their [s1, s2] window. Everything per (column, view) -- UU, Yr,
 // temp1 = sqrt(SO^2 - Yr^2), the projection slope K = SO SD/(temp1 (temp1+UU)
-// dZL), C, the channel -- is FP32, computed once and reused for the NZ slices.
+// dZL), 2^C, the channel -- is FP32, computed once and reused for the NZ slices.
 //
 // Filtered data are BF16 "pairs": word u of a detector row holds the values of
 // channels u (low half) and u+1 (high half), so one 32-bit load gives both
@@ -70,18 +72,19 @@ struct FastParams {
 
 // Per (column, view) quantities shared by the slices of a thread.
 struct ColView {
-  float K, C, fu;
+  float K, E, fu;  // E = 2^C
   int u0;
 };
 
-__device__ __forceinline__ bool col_view(const FastParams& P, float x, float y, float2 cs, ColView& cv) {
+template <class PT>
+__device__ __forceinline__ bool col_view(const PT& P, float x, float y, float2 cs, ColView& cv) {
   const float UU = -x * cs.x - y * cs.y;
   const float Yr = -x * cs.y + y * cs.x;
   const float t1sq = P.SO2 - Yr * Yr;
   const float temp1 = t1sq * rsqrtf(t1sq);
   const float A = temp1 + UU, B = temp1 - UU;
   cv.K = P.SOSDdZL * rcp_approx(temp1 * A);
-  cv.C = P.k1 * lg2_approx(B * rcp_approx(A));
+  cv.E = ex2_approx(P.k1 * lg2_approx(B * rcp_approx(A)));
   const float u1 = fmaf(Yr, P.invdYL, P.YLC0);
   float u0f;
   cv.u0 = floor_magic(u1, u0f);
@@ -105,15 +108,15 @@ __device__ __forceinline__ float blend(uint32_t w0, uint32_t w1, float fu, float
 // Per-scan table pointers of the fast backprojection.
 struct ZTabs {
   const float2* trig;     // per view: {cos, sin}
-  const float2* ztab;     // per z block and view of its window: NZ x {t2, Q}
+  const float2* ztab;     // per z block and view of its window: NZ x {t2, 2^Q}
   const uint32_t* zmask;  // per z block and view: slices whose window holds the view
   const int2* zblock;     // per z block: {first view, number of views}
   const int* zoff;        // per z block: table row of its first view
 };
 
-template <int NZ, int CH>
+template <int NZ, int CH, class PT>
 __device__ __forceinline__ void fast_column(float* __restrict__ vol, const uint32_t* __restrict__ fpb,
-                                            const ZTabs& T, const FastParams& P, int xi, int yi, int b) {
+                                            const ZTabs& T, const PT& P, int xi, int yi, int b) {
   const float2* __restrict__ trig = T.trig;
   const float2* __restrict__ ztab = T.ztab;
   const uint32_t* __restrict__ zmask = T.zmask;
@@ -125,7 +128,9 @@ __device__ __forceinline__ void fast_column(float* __restrict__ vol, const uint3
   float res[NZ];
 #pragma unroll
   for (int m = 0; m < NZ; ++m) res[m] = 0.0f;
-  const size_t plane = (size_t)P.ZL * P.YL;
+  const int pYL = P.YL, pZL = P.ZL;  // per-update constants, kept in registers
+  const float pZLC0 = P.ZLC0;
+  const size_t plane = (size_t)pZL * pYL;
   const float2* btab = ztab + (size_t)off * NZ;
   const uint32_t* bmask = zmask + off;
   for (int q = 0; q < blk.y; ++q) {
@@ -140,14 +145,14 @@ __device__ __forceinline__ void fast_column(float* __restrict__ vol, const uint3
 #pragma unroll
       for (int m = 0; m < NZ; ++m) {
         if (!(mask & (1u << m))) continue;
-        const float2 tq = __ldg(e + m);  // {t2, Q}
+        const float2 tq = __ldg(e + m);  // {t2, 2^Q}
         float v0f;
-        const float v1 = fmaf(tq.x, cv.K, P.ZLC0);
+        const float v1 = fmaf(tq.x, cv.K, pZLC0);
         const int v0 = floor_magic(v1, v0f);
-        if ((unsigned)v0 > (unsigned)(P.ZL - 2)) continue;
-        const uint32_t w0 = __ldg(col + (size_t)v0 * P.YL);
-        const uint32_t w1 = __ldg(col + (size_t)(v0 + 1) * P.YL);
-        const float wgt = rcp_approx(1.0f + ex2_approx(tq.y + cv.C));
+        if ((unsigned)v0 > (unsigned)(pZL - 2)) continue;
+        const uint32_t w0 = __ldg(col + (size_t)v0 * pYL);
+        const uint32_t w1 = __ldg(col + (size_t)(v0 + 1) * pYL);
+        const float wgt = rcp_approx(fmaf(tq.y, cv.E, 1.0f));
         res[m] = fmaf(wgt, blend(w0, w1, cv.fu, v1 - v0f), res[m]);
       }
     } else {
@@ -161,27 +166,27 @@ __device__ __forceinline__ void fast_column(float* __restrict__ vol, const uint3
         bool ok[CH];
 #pragma unroll
         for (int i = 0; i < CH; i += 2) {
-          const float4 t = __ldg(e4 + (c * CH + i) / 2);  // {t2, Q} of two slices
+          const float4 t = __ldg(e4 + (c * CH + i) / 2);  // {t2, 2^Q} of two slices
           t2[i] = t.x; qv[i] = t.y; t2[i + 1] = t.z; qv[i + 1] = t.w;
         }
 #pragma unroll
         for (int i = 0; i < CH; ++i) {
           float v0f;
-          const float v1 = fmaf(t2[i], cv.K, P.ZLC0);
+          const float v1 = fmaf(t2[i], cv.K, pZLC0);
           const int v0 = floor_magic(v1, v0f);
-          ok[i] = ((cm >> i) & 1u) && (unsigned)v0 <= (unsigned)(P.ZL - 2);
+          ok[i] = ((cm >> i) & 1u) && (unsigned)v0 <= (unsigned)(pZL - 2);
           vrow[i] = ok[i] ? v0 : 0;
           fz[i] = v1 - v0f;
         }
         uint32_t w0[CH], w1[CH];
 #pragma unroll
         for (int i = 0; i < CH; ++i) {
-          w0[i] = __ldg(col + (size_t)vrow[i] * P.YL);
-          w1[i] = __ldg(col + (size_t)(vrow[i] + 1) * P.YL);
+          w0[i] = __ldg(col + (size_t)vrow[i] * pYL);
+          w1[i] = __ldg(col + (size_t)(vrow[i] + 1) * pYL);
         }
 #pragma unroll
         for (int i = 0; i < CH; ++i) {
-          const float wgt = ok[i] ? rcp_approx(1.0f + ex2_approx(qv[i] + cv.C)) : 0.0f;
+          const float wgt = ok[i] ? rcp_approx(fmaf(qv[i], cv.E, 1.0f)) : 0.0f;
           res[c * CH + i] = fmaf(wgt, blend(w0[i], w1[i], cv.fu, fz[i]), res[c * CH + i]);
         }
       }
@@ -223,9 +228,9 @@ __device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
 // accumulation; the two table entries come in one 128-bit load and the
 // window test is one uniform branch per pair. Same operations per (voxel,
 // view) as bp_fast_kernel, in the same view order.
-template <int NZ>
+template <int NZ, class PT>
 __device__ __forceinline__ void fast_column_pairs(float* __restrict__ vol, const uint32_t* __restrict__ fpb,
-                                                  const ZTabs& T, const FastParams& P, int xi, int yi, int b) {
+                                                  const ZTabs& T, const PT& P, int xi, int yi, int b) {
   static_assert(NZ % 2 == 0, "slices are processed in pairs");
   const float2* __restrict__ trig = T.trig;
   const float2* __restrict__ ztab = T.ztab;
@@ -238,7 +243,8 @@ __device__ __forceinline__ void fast_column_pairs(float* __restrict__ vol, const
   uint64_t res[NZ / 2];
 #pragma unroll
   for (int c = 0; c < NZ / 2; ++c) res[c] = 0ull;
-  const size_t plane = (size_t)P.ZL * P.YL;
+  const int pYL = P.YL;
+  const size_t plane = (size_t)P.ZL * pYL;
   const float4* btab = reinterpret_cast<const float4*>(ztab + (size_t)off * NZ);
   const uint32_t* bmask = zmask + off;
   const uint64_t half2 = pk2(-0.49999997f, -0.49999997f), magic2 = pk2(kMagic, kMagic);
@@ -253,12 +259,12 @@ __device__ __forceinline__ void fast_column_pairs(float* __restrict__ vol, const
     if (!col_view(P, x, y, __ldg(trig + p), cv)) continue;
     const uint32_t* col = fpb + (size_t)p * plane + cv.u0;
     const float4* e = btab + (size_t)q * (NZ / 2);
-    const uint64_t k2 = pk2(cv.K, cv.K), c2 = pk2(cv.C, cv.C), fu2 = pk2(cv.fu, cv.fu);
+    const uint64_t k2 = pk2(cv.K, cv.K), e2 = pk2(cv.E, cv.E), fu2 = pk2(cv.fu, cv.fu);
 #pragma unroll
     for (int c = 0; c < NZ / 2; ++c) {
       const uint32_t pm = (mask >> (2 * c)) & 3u;
       if (pm == 0u) continue;  // uniform over the CTA
-      const float4 t = __ldg(e + c);  // {t2, Q} of slices 2c and 2c+1
+      const float4 t = __ldg(e + c);  // {t2, 2^Q} of slices 2c and 2c+1
       const uint64_t v1 = fma2(pk2(t.x, t.z), k2, zlc2);
       const uint64_t r = add2(add2(v1, half2), magic2);  // round(v1 - 1/2) in the low mantissa bits
       const uint64_t v0f = sub2(r, magic2);
@@ -268,10 +274,10 @@ __device__ __forceinline__ void fast_column_pairs(float* __restrict__ vol, const
       const int va = __float_as_int(ra_) - 0x4B400000, vb = __float_as_int(rb_) - 0x4B400000;
       const bool oka = (pm & 1u) && (unsigned)va <= vmax;
       const bool okb = (pm & 2u) && (unsigned)vb <= vmax;
-      const uint32_t* ca = col + (size_t)(oka ? va : 0) * P.YL;
-      const uint32_t* cb = col + (size_t)(okb ? vb : 0) * P.YL;
-      const uint32_t wa0 = __ldg(ca), wa1 = __ldg(ca + P.YL);
-      const uint32_t wb0 = __ldg(cb), wb1 = __ldg(cb + P.YL);
+      const uint32_t* ca = col + (size_t)(oka ? va : 0) * pYL;
+      const uint32_t* cb = col + (size_t)(okb ? vb : 0) * pYL;
+      const uint32_t wa0 = __ldg(ca), wa1 = __ldg(ca + pYL);
+      const uint32_t wb0 = __ldg(cb), wb1 = __ldg(cb + pYL);
       // (slice a, slice b) lanes: row V0 taps u, u+1 and row V0+1 taps u, u+1
       const uint64_t r0u0 = pk2(__uint_as_float(wa0 << 16), __uint_as_float(wb0 << 16));
       const uint64_t r0u1 = pk2(__uint_as_float(wa0 & 0xffff0000u), __uint_as_float(wb0 & 0xffff0000u));
@@ -280,10 +286,8 @@ __device__ __forceinline__ void fast_column_pairs(float* __restrict__ vol, const
       const uint64_t ra = fma2(fu2, sub2(r0u1, r0u0), r0u0);
       const uint64_t rb = fma2(fu2, sub2(r1u1, r1u0), r1u0);
       const uint64_t tap = fma2(fz, sub2(rb, ra), ra);
-      float xa, xb;
-      up2(add2(pk2(t.y, t.w), c2), xa, xb);
       float sa, sb;
-      up2(add2(pk2(ex2_approx(xa), ex2_approx(xb)), one2), sa, sb);
+      up2(fma2(pk2(t.y, t.w), e2, one2), sa, sb);
       const uint64_t wgt = pk2(oka ? rcp_approx(sa) : 0.0f, okb ? rcp_approx(sb) : 0.0f);
       res[c] = fma2(wgt, tap, res[c]);
     }
@@ -299,13 +303,13 @@ __device__ __forceinline__ void fast_column_pairs(float* __restrict__ vol, const
 }
 
 // CH >= 0: fast_column<NZ, CH>; CH < 0: slice pairs in packed FP32x2.
-template <int NZ, int CH>
-__device__ __forceinline__ void column(float* vol, const uint32_t* fpb, const ZTabs& T, const FastParams& P, int xi,
-                                       int yi, int b) {
+template <int NZ, int CH, class PT = FastParams>
+__device__ __forceinline__ void column(float* vol, const uint32_t* fpb, const ZTabs& T, const PT& P, int xi, int yi,
+                                       int b) {
   if constexpr (CH < 0)
-    fast_column_pairs<NZ>(vol, fpb, T, P, xi, yi, b);
+    fast_column_pairs<NZ, PT>(vol, fpb, T, P, xi, yi, b);
   else
-    fast_column<NZ, CH>(vol, fpb, T, P, xi, yi, b);
+    fast_column<NZ, CH, PT>(vol, fpb, T, P, xi, yi, b);
 }
 
 // One CTA per (8 x 16 column tile, z block); grid z covers z blocks
@@ -453,7 +457,7 @@ static int build_host(BpFastHostSet* t, int NZ, const BpFastGeom& g, const doubl
         const double tc = p < s0[zi] ? t2 - 0.5 : t2 + 0.5;
         double Q = g.k1 * (std::log2(std::fabs(t2)) - std::log2(std::fabs(tc)));
         Q += std::log2(w[d2]) - std::log2(w[d1]);
-        t->tab[row * NZ + m] = make_float2((float)t2, (float)Q);
+        t->tab[row * NZ + m] = make_float2((float)t2, (float)std::exp2(Q));
         mk |= 1u << m;
       }
       t->mask[row] = mk;

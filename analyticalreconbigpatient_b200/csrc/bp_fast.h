@@ -41,7 +41,7 @@ constexpr int kBatchMaxScans = 16;
 struct BpFastTables {
   int nz = 0, nblocks = 0;
   size_t cap_rows = 0;         // reserved table rows (views summed over blocks)
-  float2* d_tab = nullptr;     // per z block and view of its window: NZ x {t2, Q}
+  float2* d_tab = nullptr;     // per z block and view of its window: NZ x {t2, 2^Q}
   uint32_t* d_mask = nullptr;  // per z block and view: slices whose [s1, s2] holds the view
   int* d_zblock = nullptr;     // [nblocks] {first view, count}, then [nblocks] table offsets
   size_t bytes = 0;

@@ -230,3 +230,42 @@ def evaluate(net: Corrector, data: PairSet, chunk: int = 8) -> dict:
             n += pred.numel()
     return {"hu_rmse_learned": math.sqrt(sq_net / n) / MU_WATER * 1000.0,
             "hu_rmse_half_view": math.sqrt(sq_plain / n) / MU_WATER * 1000.0, "slices": n // (H * W)}
+
+
+def main(argv=None) -> None:
+    """Train on seeded phantoms and evaluate on held-out ones from the command line:
+    python -m analyticalreconbigpatient_b200.learned --phantoms 200 --steps 600 --eval 20 [--save params.npy]"""
+    import argparse
+    import json
+    import time
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--phantoms", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--eval", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--grid", type=int, default=512)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--save", default=None, help="write the trained parameters (.npy)")
+    a = ap.parse_args(argv)
+    pixel = 0.9766 * 512 / a.grid
+    t0 = time.perf_counter()
+    train_set = PairSet(range(1, 1 + a.phantoms), grid=a.grid, pixel=pixel)
+    t1 = time.perf_counter()
+    net = Corrector(seed=a.seed)
+    losses = train(net, train_set, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    del train_set
+    test_set = PairSet(range(100001, 100001 + a.eval), grid=a.grid, pixel=pixel)
+    ev = evaluate(net, test_set)
+    if a.save:
+        np.save(a.save, net.params())
+    print(json.dumps({"data_s": t1 - t0, "train_s": t2 - t1, "loss_first": float(np.mean(losses[:20])),
+                      "loss_last": float(np.mean(losses[-20:])), **ev}), flush=True)
+    net.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-slab", type=int, default=128,
+                    help="fast form: also time e2e through the slab pipeline with slabs of this many slices "
+                         "(0: off); the faster entry is reported")
     return ap.parse_args()
 
 
@@ -324,6 +327,33 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
             dist.all_reduce(tm, op=dist.ReduceOp.MAX)
             e2e_s = float(tm.item())
         out["e2e_s"] = e2e_s
+        out["e2e_entry"] = "hr_recon_execute_host (C ABI, pinned host buffers)"
+        if fast and args.e2e_slab > 0:
+            # the same volume through the slab pipeline: host-to-device copies of later slabs' fan windows
+            # overlap the reconstruction of earlier slabs (hr_slab_execute with host buffers)
+            from analyticalreconbigpatient_b200.pipeline import SlabRecon
+
+            rec.close()
+            torch.cuda.empty_cache()
+            slab = SlabRecon(scan, slab_slices=args.e2e_slab, device=dev)
+            slab.run(h_fan, h_vol)  # warm (autotunes, captures)
+            barrier()
+            slab_t = []
+            for _ in range(args.e2e_steps):
+                t = time.perf_counter()
+                slab.run(h_fan, h_vol)
+                slab_t.append(time.perf_counter() - t)
+            slab_s = statistics.median(slab_t)
+            if world > 1:
+                tm = torch.tensor([slab_s], device=dev)
+                dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+                slab_s = float(tm.item())
+            out["e2e_chain_s"] = e2e_s
+            out["e2e_slab_s"] = slab_s
+            slab.close()
+            if slab_s < e2e_s:
+                out["e2e_s"] = slab_s
+                out["e2e_entry"] = f"hr_slab_execute (C ABI, pinned host buffers, z slabs of {args.e2e_slab})"
         del h_fan, h_vol
     rec.close()
     torch.cuda.empty_cache()
@@ -583,52 +613,60 @@ def run_learned(args, dev, world, rank, barrier):
     h_half.copy_(fan[::2])
     del fan
     rf = HelicalRecon(full, form=_lib.HR_FORM_PLAIN, device=dev)
-    rh = HelicalRecon(half, form=_lib.HR_FORM_PLAIN, device=dev)
+    # the half view is reconstructed with the chosen (fast) form; the plain form beside it
+    rh = {"fast": HelicalRecon(half, form=_lib.HR_FORM_FAST, device=dev),
+          "plain": HelicalRecon(half, form=_lib.HR_FORM_PLAIN, device=dev)}
     d_half = torch.empty(h_half.shape, dtype=torch.float32, device=dev)
-    v_half = torch.empty((half.YN, half.XN, half.ZN), dtype=torch.float32, device=dev)
-    v_out = torch.empty_like(v_half)
-    h_out = torch.empty(v_half.shape, dtype=torch.float32, pin_memory=True)
-    h_ref = torch.empty(v_half.shape, dtype=torch.float32, pin_memory=True)
+    v_half = {k: torch.empty((half.YN, half.XN, half.ZN), dtype=torch.float32, device=dev) for k in rh}
+    v_out = {k: torch.empty_like(v_half[k]) for k in rh}
+    h_out = torch.empty((half.YN, half.XN, half.ZN), dtype=torch.float32, pin_memory=True)
+    h_ref = torch.empty_like(h_out, pin_memory=True)
 
-    def learned_step():
+    def learned_step(kind):
         d_half.copy_(h_half, non_blocking=True)
-        rh.run(d_half, v_half)
-        net.apply_volume(v_half, v_out)
-        h_out.copy_(v_out, non_blocking=True)
+        rh[kind].run(d_half, v_half[kind])
+        net.apply_volume(v_half[kind], v_out[kind])
+        h_out.copy_(v_out[kind], non_blocking=True)
         torch.cuda.synchronize()
 
     def full_step():
         rf.run_host(h_full, h_ref)
 
     for _ in range(args.warmup):
-        learned_step()
+        learned_step("fast")
+        learned_step("plain")
         full_step()
     barrier()
     clocks = ClockSampler(None)
     clocks.start()
-    tl, tf, tc = [], [], []
+    tl, tlp, tf, tc = [], [], [], []
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for _ in range(args.steps):
         t = time.perf_counter()
-        learned_step()
+        learned_step("fast")
         tl.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        learned_step("plain")
+        tlp.append(time.perf_counter() - t)
         t = time.perf_counter()
         full_step()
         tf.append(time.perf_counter() - t)
         e0.record(stream)
-        net.apply_volume(v_half, v_out)
+        net.apply_volume(v_half["fast"], v_out["fast"])
         e1.record(stream)
         torch.cuda.synchronize()
         tc.append(e0.elapsed_time(e1))
     clocks.stop()
-    s_learned, s_full = statistics.median(tl), statistics.median(tf)
+    s_learned, s_learned_plain, s_full = statistics.median(tl), statistics.median(tlp), statistics.median(tf)
     cnn_ms = statistics.median(tc)
     ref = h_ref.to(dev)
-    hu_learned, hu_half = L.hu_rmse(v_out, ref), L.hu_rmse(v_half, ref)
+    hu = {k: (L.hu_rmse(v_out[k], ref), L.hu_rmse(v_half[k], ref)) for k in rh}
+    hu_learned, hu_half = hu["fast"]
     net.check()
     rf.close()
-    rh.close()
+    for r in rh.values():
+        r.close()
     # network FLOPs per slice: 2 * pixels * sum(9 * cin * cout) (padded channels counted)
     flops = 2.0 * half.XN * half.YN * sum(9 * ci * co for ci, co in zip(L.CIN, L.COUT)) * half.ZN
     pk, pk_kind = peaks()
@@ -639,7 +677,7 @@ def run_learned(args, dev, world, rank, barrier):
             "warmup": args.warmup, "ms_per_step": s_learned * 1e3, "s_per_volume": s_learned,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
             "data": "synthetic (seeded random-ellipsoid phantoms, Poisson noise at I0=1e5)",
-            "form": "learned (half-view plain + 2.5D CNN)",
+            "form": "learned (half-view fast reconstruction + 2.5D CNN)",
             "config": {"workload": f"helical 888x64, pitch 0.984, 10 rot at 492 views/rot (every second view of "
                                    f"the 984-view scan) -> 512x512x{half.ZN} @ 0.9766x0.9766x0.625 mm",
                        "updates_per_volume": upd_half, "flush": "inputs larger than L2 (1.1 GB of fan data)"},
@@ -648,7 +686,10 @@ def run_learned(args, dev, world, rank, barrier):
                         "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:])),
                         "held_out_phantoms": args.eval_phantoms, **ev,
                         "volume_hu_rmse_learned": hu_learned, "volume_hu_rmse_half_view": hu_half,
-                        "s_per_volume_learned": s_learned, "s_per_volume_full_view_plain": s_full,
+                        "volume_hu_rmse_learned_on_plain_half": hu["plain"][0],
+                        "volume_hu_rmse_plain_half_view": hu["plain"][1],
+                        "s_per_volume_learned": s_learned, "s_per_volume_learned_on_plain_half": s_learned_plain,
+                        "s_per_volume_full_view_plain": s_full,
                         "speedup_vs_full_view_plain": s_full / s_learned, "cnn_ms_per_volume": cnn_ms},
             "roofline": {"bound": "tensor", "kernel": "conv_tc_kernel (8 layers, whole volume)", "achieved": tflops,
                          "peak": pk["bf16_tflops"], "unit": "TFLOP/s", "frac": tflops / pk["bf16_tflops"],
@@ -657,7 +698,7 @@ def run_learned(args, dev, world, rank, barrier):
                                  "bound by activation traffic (32 channels: 144 FLOP per byte)"},
             "e2e": {"value": upd_half * world / s_learned / 1e9, "unit": "GUPS", "s_per_volume": s_learned,
                     "h2d_bytes_per_step": half.projection_bytes(), "d2h_bytes_per_step": half.volume_bytes(),
-                    "entry": "HelicalRecon.run + Corrector.apply_volume, pinned host fan in, volume out"},
+                    "entry": "HelicalRecon.run (fast form) + Corrector.apply_volume, pinned host fan in, volume out"},
             "gpu_launches": None, "clocks": clocks.summary()}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -754,7 +795,8 @@ def main():
             "roofline": roofline,
             "e2e": {"value": e2e_value, "unit": "GUPS", "s_per_volume": res["e2e_s"],
                     "h2d_bytes_per_step": scan.projection_bytes(), "d2h_bytes_per_step": scan.volume_bytes(),
-                    "entry": "hr_recon_execute_host (C ABI, pinned host buffers)"},
+                    "entry": res["e2e_entry"],
+                    **({"chain_s": res["e2e_chain_s"], "slab_s": res["e2e_slab_s"]} if "e2e_slab_s" in res else {})},
             "gpu_launches": res["launches_per_step"] * args.steps,
             "kernels": res["kernels"],
             "clocks": clocks.summary()}
