@@ -39,6 +39,25 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def max_over_ranks(values, world: int, device):
+    """Element-wise maximum over the ranks of a job (a multi-GPU step takes as long as its slowest
+    rank); the values of a single process are returned unchanged."""
+    values = [float(v) for v in values]
+    if world <= 1:
+        return values
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def job_gups(updates_per_rank: int, world: int, seconds: float) -> float:
+    """Whole-job throughput: every rank reconstructs its own scan of the same size (weak scaling)."""
+    return updates_per_rank * world / seconds / 1e9
 BYTES_PER_UPDATE_FP32 = 16  # four FP32 taps per voxel-view update
 BYTES_PER_UPDATE_BF16 = 8   # four BF16 taps per voxel-view update
 
@@ -301,10 +320,7 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
     barrier()
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1) / args.steps
-    if world > 1:
-        tm = torch.tensor([ms], device=dev)
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        ms = float(tm.item())
+    (ms,) = max_over_ranks([ms], world, dev)
     rec.check()
     out = {"ms_per_step": ms, "stages_ms": {k: statistics.mean(v) for k, v in stage_ms.items() if v},
            "launches_per_step": 4 if fast else 3, "kernels": rec.describe()}
@@ -322,10 +338,7 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
             rec.run_host(h_fan, h_vol)
             e2e_t.append(time.perf_counter() - t)
         e2e_s = statistics.median(e2e_t)
-        if world > 1:
-            tm = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-            e2e_s = float(tm.item())
+        (e2e_s,) = max_over_ranks([e2e_s], world, dev)
         out["e2e_s"] = e2e_s
         out["e2e_entry"] = "hr_recon_execute_host (C ABI, pinned host buffers)"
         if fast and args.e2e_slab > 0:
@@ -344,10 +357,7 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
                 slab.run(h_fan, h_vol)
                 slab_t.append(time.perf_counter() - t)
             slab_s = statistics.median(slab_t)
-            if world > 1:
-                tm = torch.tensor([slab_s], device=dev)
-                dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-                slab_s = float(tm.item())
+            (slab_s,) = max_over_ranks([slab_s], world, dev)
             out["e2e_chain_s"] = e2e_s
             out["e2e_slab_s"] = slab_s
             slab.close()
@@ -391,10 +401,7 @@ def run_bigpatient(args, scan, dev, world, rank, barrier):
     torch.cuda.synchronize()
     clocks.stop()
     ms = t0.elapsed_time(t1) / args.steps
-    if world > 1:
-        tm = torch.tensor([ms], device=dev)
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        ms = float(tm.item())
+    (ms,) = max_over_ranks([ms], world, dev)
     desc = rec.describe()
     updates = scan.updates()
     # e2e from host memory (pinned if the host allows it)
@@ -413,7 +420,7 @@ def run_bigpatient(args, scan, dev, world, rank, barrier):
         t = time.perf_counter()
         rec.run(h_fan, h_vol)
         e2e_t.append(time.perf_counter() - t)
-    e2e_s = statistics.median(e2e_t)
+    (e2e_s,) = max_over_ranks([statistics.median(e2e_t)], world, dev)
     rec.close()
     # backprojection roofline from the autotuner's best measured time per slice (same process)
     import re
@@ -490,10 +497,7 @@ def run_batch(args, dev, world, rank, barrier):
     t1.record(stream)
     torch.cuda.synchronize()
     bp_ms = t0.elapsed_time(t1) / args.steps
-    if world > 1:
-        tm = torch.tensor([ms, bp_ms], device=dev)
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        ms, bp_ms = (float(v) for v in tm.tolist())
+    ms, bp_ms = max_over_ranks([ms, bp_ms], world, dev)
     desc = rec.describe()
     batch_vols = [v.cpu() for v in vols]
     # e2e: pinned host fans in, volumes out, every step
@@ -658,8 +662,8 @@ def run_learned(args, dev, world, rank, barrier):
         torch.cuda.synchronize()
         tc.append(e0.elapsed_time(e1))
     clocks.stop()
-    s_learned, s_learned_plain, s_full = statistics.median(tl), statistics.median(tlp), statistics.median(tf)
-    cnn_ms = statistics.median(tc)
+    s_learned, s_learned_plain, s_full, cnn_ms = max_over_ranks(
+        [statistics.median(tl), statistics.median(tlp), statistics.median(tf), statistics.median(tc)], world, dev)
     ref = h_ref.to(dev)
     hu = {k: (L.hu_rmse(v_out[k], ref), L.hu_rmse(v_half[k], ref)) for k in rh}
     hu_learned, hu_half = hu["fast"]
@@ -699,7 +703,9 @@ def run_learned(args, dev, world, rank, barrier):
             "e2e": {"value": upd_half * world / s_learned / 1e9, "unit": "GUPS", "s_per_volume": s_learned,
                     "h2d_bytes_per_step": half.projection_bytes(), "d2h_bytes_per_step": half.volume_bytes(),
                     "entry": "HelicalRecon.run (fast form) + Corrector.apply_volume, pinned host fan in, volume out"},
-            "gpu_launches": None, "clocks": clocks.summary()}
+            # per learned step: rebin, split, Toeplitz GEMM, backprojection; then per 32-slice chunk the
+            # input packing and 8 conv layers
+            "gpu_launches": (4 + 9 * ((half.ZN + 31) // 32)) * args.steps, "clocks": clocks.summary()}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
