@@ -42,7 +42,7 @@ constexpr int kTileM = 128;                  // output pixels per tile (one row 
 constexpr int kHalo = kTileM + 2;            // halo pixels per row
 constexpr int kBox = kHalo * 16;             // bytes of one TMA box: 8 channels x 130 pixels
 constexpr int kPlane = 17 * 128;             // plane stride: one box, 128-byte aligned
-constexpr int kStages = 3;                   // halo ring
+constexpr int kRing = 6;                     // halo ring: input rows in flight
 constexpr int kThreads = 192;                // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr int kTmemCols = 64;                // two 32-column accumulators
 constexpr uint32_t kWaitLimit = 1u << 22;    // try_wait rounds before a wait is declared hung
@@ -180,35 +180,37 @@ struct ConvArgs {
   float grad_scale;      // EPI_LOSS: d loss / d r = grad_scale * (pred - target) / scale
   float* loss;           // EPI_LOSS: accumulates sum ((pred - target) / scale)^2
   int B, H, W;
+  int rows_per_unit;     // output rows a CTA computes down one 128-pixel column strip
   int* err;
 };
 
 template <int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant__ ConvArgs a) {
-  constexpr int G = CIN / 8;                 // 8-channel groups (TMA boxes per halo row)
-  constexpr int kRow = G * kPlane;           // bytes of one halo row
-  constexpr int kStageBytes = 3 * kRow;
+  constexpr int G = CIN / 8;                 // 8-channel groups (TMA boxes per input row)
+  constexpr int kRow = G * kPlane;           // bytes of one input row (130 pixels)
   constexpr int kWBytes = 9 * CIN * COUT * 2;
   constexpr int kKSteps = 9 * CIN / 16;
   constexpr uint32_t kIdesc = idesc_bf16(COUT);
-  constexpr uint32_t kTxBytes = 3 * G * kBox;
+  constexpr uint32_t kTxBytes = G * kBox;
   static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "unsupported channel counts");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-  uint8_t* wsm = smem + kStages * kStageBytes;  // weights
+  uint8_t* wsm = smem + kRing * kRow;  // weights
   uint64_t* full = reinterpret_cast<uint64_t*>(wsm + kWBytes);
-  uint64_t* empty = full + kStages;
-  uint64_t* tfull = empty + kStages;
+  uint64_t* empty = full + kRing;
+  uint64_t* tfull = empty + kRing;
   uint64_t* tempty = tfull + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  float* bias_s = reinterpret_cast<float*>(tmem_slot + 4);  // 16-byte aligned, COUT floats
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int i = tid; i < kWBytes / 16; i += kThreads)
     reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.wimg) + i);
+  if (tid < COUT) bias_s[tid] = a.bias ? __ldg(a.bias + tid) : 0.0f;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < kRing; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -229,63 +231,90 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
   const uint32_t tmem = *tmem_slot;
   const uint32_t smem_a = smem_u32(smem), w_a = smem_u32(wsm);
 
+  // Work units: (image b, 128-pixel column strip seg, chunk of rows_per_unit output rows). Down a
+  // strip each input row is loaded once into the ring and serves three consecutive output rows;
+  // a unit of n output rows loads n + 2 input rows (zero rows above and below the image).
   const int nseg = (a.W + kTileM - 1) / kTileM;
-  const long long tiles = (long long)a.B * a.H * nseg;
+  const int rpu = a.rows_per_unit;
+  const int nchunk = (a.H + rpu - 1) / rpu;
+  const long long units = (long long)a.B * nseg * nchunk;
   if (warp == 0) {
-    // ---- producer: the halo of each tile, 3 rows x G boxes --------------------------------
+    // ---- producer: input rows of each unit into the ring, G boxes per row --------------------
     if (lane == 0) {
-      int it = 0;
-      for (long long t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
-        const int s = it % kStages;
-        if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, abort_flag, a.err)) break;
-        const int seg = (int)(t % nseg);
-        const long long by = t / nseg;
-        const int y = (int)(by % a.H), b = (int)(by / a.H);
-        mbar_expect_tx(&full[s], kTxBytes);
-        const uint32_t st = smem_a + s * kStageBytes;
-        for (int r = 0; r < 3; ++r)
+      int h = 0;  // input rows loaded by this CTA
+      bool ok = true;
+      for (long long un = blockIdx.x; un < units && ok; un += gridDim.x) {
+        const int seg = (int)(un % nseg), chunk = (int)((un / nseg) % nchunk), b = (int)(un / ((long long)nseg * nchunk));
+        const int y0 = chunk * rpu, ny = min(rpu, a.H - y0);
+        for (int j = 0; j < ny + 2; ++j, ++h) {
+          const int s = h % kRing;
+          if (h >= kRing && !mbar_wait(&empty[s], ((h / kRing) - 1) & 1, abort_flag, a.err)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&full[s], kTxBytes);
           for (int g = 0; g < G; ++g)
-            tma_load_4d(st + r * kRow + g * kPlane, &a.in_map, &full[s], g * 8, seg * kTileM - 1, y + r - 1, b);
+            tma_load_4d(smem_a + s * kRow + g * kPlane, &a.in_map, &full[s], g * 8, seg * kTileM - 1, y0 - 1 + j, b);
+        }
       }
     }
   } else if (warp == 1) {
-    // ---- MMA issuer --------------------------------------------------------------------------
+    // ---- MMA issuer: output row i of a unit reads input rows i, i+1, i+2 of the unit ---------
     if (lane == 0) {
-      int it = 0;
-      for (long long t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
-        const int s = it % kStages, acc = it & 1;
-        if (!mbar_wait(&full[s], (it / kStages) & 1, abort_flag, a.err)) break;
-        if (it >= 2 && !mbar_wait(&tempty[acc], ((it >> 1) - 1) & 1, abort_flag, a.err)) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t st = smem_a + s * kStageBytes;
+      int hbase = 0, o = 0;
+      bool ok = true;
+      for (long long un = blockIdx.x; un < units && ok; un += gridDim.x) {
+        const int chunk = (int)((un / nseg) % nchunk);
+        const int ny = min(rpu, a.H - chunk * rpu);
+        for (int i = 0; i < ny && ok; ++i, ++o) {
+          for (int j = (i == 0 ? 0 : 2); j < 3 && ok; ++j) {
+            const int hh = hbase + i + j;
+            ok = mbar_wait(&full[hh % kRing], (hh / kRing) & 1, abort_flag, a.err);
+          }
+          const int acc = o & 1;
+          if (ok && o >= 2) ok = mbar_wait(&tempty[acc], ((o >> 1) - 1) & 1, abort_flag, a.err);
+          if (!ok) break;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-        for (int k = 0; k < kKSteps; ++k) {
-          const int k0 = k * 16;
-          const int tap = k0 / CIN, c0 = k0 - tap * CIN;
-          const int dy = tap / 3, dx = tap - dy * 3;  // halo row and pixel offset
-          const uint64_t ad = desc_noswz(st + dy * kRow + (c0 / 8) * kPlane + dx * 16, kPlane, 128);
-          const uint64_t bd = desc_noswz(w_a + (k0 / 8) * (COUT * 16), COUT * 16, 128);
-          umma(tmem + acc * 32, ad, bd, kIdesc, k > 0 ? 1u : 0u);
+          for (int k = 0; k < kKSteps; ++k) {
+            const int k0 = k * 16;
+            const int tap = k0 / CIN, c0 = k0 - tap * CIN;
+            const int dy = tap / 3, dx = tap - dy * 3;  // input row and pixel offset
+            const uint32_t row = smem_a + ((hbase + i + dy) % kRing) * kRow;
+            const uint64_t ad = desc_noswz(row + (c0 / 8) * kPlane + dx * 16, kPlane, 128);
+            const uint64_t bd = desc_noswz(w_a + (k0 / 8) * (COUT * 16), COUT * 16, 128);
+            umma(tmem + acc * 32, ad, bd, kIdesc, k > 0 ? 1u : 0u);
+          }
+          umma_commit(&tfull[acc]);                       // the accumulator is ready
+          umma_commit(&empty[(hbase + i) % kRing]);        // input row i serves no later output row
+          if (i == ny - 1) {
+            umma_commit(&empty[(hbase + i + 1) % kRing]);  // the unit's last two input rows
+            umma_commit(&empty[(hbase + i + 2) % kRing]);
+          }
         }
-        umma_commit(&empty[s]);    // the halo stage may be refilled
-        umma_commit(&tfull[acc]);  // the accumulator is ready
+        hbase += ny + 2;
       }
     }
   } else {
     // ---- epilogue: warps 2-5, TMEM lane quarter warp % 4 --------------------------------------
     const int q = warp & 3;
     int it = 0;
-    for (long long t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+    bool ok = true;
+    for (long long un = blockIdx.x; un < units && ok; un += gridDim.x) {
+     const int seg = (int)(un % nseg), chunk = (int)((un / nseg) % nchunk), b = (int)(un / ((long long)nseg * nchunk));
+     const int y0 = chunk * rpu, ny = min(rpu, a.H - y0);
+     for (int i = 0; i < ny; ++i, ++it) {
       const int acc = it & 1;
-      if (!mbar_wait(&tfull[acc], (it >> 1) & 1, abort_flag, a.err)) break;
+      if (!mbar_wait(&tfull[acc], (it >> 1) & 1, abort_flag, a.err)) {
+        ok = false;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       float v[COUT];
       tmem_ld<COUT>(tmem + acc * 32 + ((uint32_t)(q * 32) << 16), v);
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&tempty[acc]);  // the registers hold the tile: the accumulator may be reused
-      const int seg = (int)(t % nseg);
-      const long long by = t / nseg;
-      const int y = (int)(by % a.H), b = (int)(by / a.H);
+      const int y = y0 + i;
       const int x = seg * kTileM + q * 32 + lane;
       const bool valid = x < a.W;
       const size_t pix = ((size_t)b * a.H + y) * a.W + x;
@@ -296,7 +325,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
           for (int c = 0; c < COUT / 8; ++c) {
             float u[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) u[j] = fmaxf(v[8 * c + j] + __ldg(a.bias + 8 * c + j), 0.0f);
+            for (int j = 0; j < 8; ++j) u[j] = fmaxf(v[8 * c + j] + bias_s[8 * c + j], 0.0f);
             o[c] = make_uint4(pack2(u[0], u[1]), pack2(u[2], u[3]), pack2(u[4], u[5]), pack2(u[6], u[7]));
           }
         }
@@ -318,7 +347,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
           }
         }
       } else {
-        const float r = v[0] + __ldg(a.bias);
+        const float r = v[0] + bias_s[0];
         float e2 = 0.0f;
         if (valid) {
           const size_t off = (size_t)b * a.sb + ((size_t)y * a.W + x) * a.sp;
@@ -341,6 +370,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
           if (lane == 0 && e2 != 0.0f) atomicAdd(a.loss, e2);
         }
       }
+     }
     }
   }
   __syncthreads();
@@ -515,10 +545,10 @@ int make_act_map(CUtensorMap* map, const void* base, int C, int B, int H, int W)
   return HR_OK;
 }
 
-// Dynamic shared memory of a conv CTA: halo ring + weights + barriers + alignment slack.
+// Dynamic shared memory of a conv CTA: input-row ring + weights + barriers + alignment slack.
 template <int CIN, int COUT>
 constexpr size_t conv_smem() {
-  return (size_t)kStages * 3 * (CIN / 8) * kPlane + 9 * CIN * COUT * 2 + 256 + 128;
+  return (size_t)kRing * (CIN / 8) * kPlane + 9 * CIN * COUT * 2 + 256 + COUT * 4 + 128;
 }
 
 template <int CIN, int COUT, int EPI>
@@ -527,11 +557,27 @@ int launch_conv(ConvArgs& a, cudaStream_t s) {
   HR_TRY(make_act_map(&a.in_map, a.in, CIN, a.B, a.H, a.W));
   HR_CUDA_TRY(cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
-  int per_sm = 0;
-  HR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_tc_kernel<CIN, COUT, EPI>, kThreads,
-                                                            smem));
-  const long long tiles = (long long)a.B * a.H * ((a.W + kTileM - 1) / kTileM);
-  const long long grid = std::min<long long>(tiles, (long long)std::max(per_sm, 1) * hr::sm_count());
+  // the largest shared-memory carveout, so that several CTAs (input-row rings) fit on an SM
+  HR_CUDA_TRY(cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT, EPI>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   (int)cudaSharedmemCarveoutMaxShared));
+  // resident CTAs per SM from the kernel's resources: shared memory (1 KiB reserved per CTA), TMEM
+  // columns, registers and threads. CTAs never wait on one another, so a grid larger than what is
+  // resident is only queued.
+  cudaFuncAttributes fa;
+  HR_CUDA_TRY(cudaFuncGetAttributes(&fa, conv_tc_kernel<CIN, COUT, EPI>));
+  int dev = 0, smem_sm = 0;
+  HR_CUDA_TRY(cudaGetDevice(&dev));
+  HR_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  const int by_smem = smem_sm / (int)(smem + fa.sharedSizeBytes + 1024);
+  const int by_tmem = 512 / kTmemCols;
+  const int by_regs = 65536 / std::max(1, fa.numRegs * kThreads);
+  const int per_sm = std::max(1, std::min({by_smem, by_tmem, by_regs, 2048 / kThreads}));
+  const long long ctas = (long long)per_sm * hr::sm_count();
+  // rows per unit: about four units per resident CTA (balance), at least 4 rows (each unit reloads 2 rows)
+  const long long strips = (long long)a.B * ((a.W + kTileM - 1) / kTileM);
+  a.rows_per_unit = (int)std::min<long long>(64, std::max<long long>(4, strips * a.H / (4 * ctas)));
+  const long long units = strips * ((a.H + a.rows_per_unit - 1) / a.rows_per_unit);
+  const long long grid = std::min<long long>(units, ctas);
   if (grid <= 0) return HR_OK;
   conv_tc_kernel<CIN, COUT, EPI><<<(unsigned)grid, kThreads, smem, s>>>(a);
   HR_CUDA_TRY(cudaGetLastError());
@@ -545,6 +591,8 @@ int launch_wgrad(const uint16_t* X, const uint16_t* Gr, int B, int H, int W, flo
   if (grid <= 0) return HR_OK;
   const size_t smem = sizeof(float) * (3 * kHalo * CIN + kTileM * COUT);
   HR_CUDA_TRY(cudaFuncSetAttribute(wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HR_CUDA_TRY(cudaFuncSetAttribute(wgrad_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   (int)cudaSharedmemCarveoutMaxShared));
   wgrad_kernel<CIN, COUT><<<(unsigned)grid, (COUT / 4) * CIN, smem, s>>>(X, Gr, B, H, W, dW, db);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
