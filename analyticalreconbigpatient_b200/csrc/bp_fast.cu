@@ -70,10 +70,36 @@ struct FastParams {
   float XNC, YNC, dx, dy, SO2, SOSDdZL, invdYL, YLC0, ZLC0, k1, DeltaFai;
 };
 
+// ---- packed FP32x2 arithmetic (sm_100: one instruction for two lanes) ----
+__device__ __forceinline__ uint64_t pk2(float a, float b) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void up2(uint64_t r, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
 // Per (column, view) quantities shared by the slices of a thread.
 struct ColView {
   float K, E, fu;  // E = 2^C
   int u0;
+  uint64_t fu2;    // (fu, fu) for packed row blends
 };
 
 template <class PT>
@@ -89,14 +115,18 @@ __device__ __forceinline__ bool col_view(const PT& P, float x, float y, float2 c
   float u0f;
   cv.u0 = floor_magic(u1, u0f);
   cv.fu = u1 - u0f;
+  cv.fu2 = pk2(cv.fu, cv.fu);
   return (unsigned)cv.u0 <= (unsigned)(P.YL - 2);
 }
 
-__device__ __forceinline__ float blend(uint32_t w0, uint32_t w1, float fu, float fz) {
-  const float a0 = __uint_as_float(w0 << 16), a1 = __uint_as_float(w0 & 0xffff0000u);
-  const float b0 = __uint_as_float(w1 << 16), b1 = __uint_as_float(w1 & 0xffff0000u);
-  const float ra = fmaf(fu, a1 - a0, a0);
-  const float rb = fmaf(fu, b1 - b0, b0);
+// Bilinear tap from two BF16 channel pairs (rows V0 and V0+1): the two row
+// blends run as one packed FP32x2 FMA (lane-wise the same roundings as two
+// scalar FMAs).
+__device__ __forceinline__ float blend(uint32_t w0, uint32_t w1, uint64_t fu2, float fz) {
+  const uint64_t lo = pk2(__uint_as_float(w0 << 16), __uint_as_float(w1 << 16));                  // taps u
+  const uint64_t hi = pk2(__uint_as_float(w0 & 0xffff0000u), __uint_as_float(w1 & 0xffff0000u));  // taps u+1
+  float ra, rb;
+  up2(fma2(fu2, sub2(hi, lo), lo), ra, rb);
   return fmaf(fz, rb - ra, ra);
 }
 
@@ -153,7 +183,7 @@ __device__ __forceinline__ void fast_column(float* __restrict__ vol, const uint3
         const uint32_t w0 = __ldg(col + (size_t)v0 * pYL);
         const uint32_t w1 = __ldg(col + (size_t)(v0 + 1) * pYL);
         const float wgt = rcp_approx(fmaf(tq.y, cv.E, 1.0f));
-        res[m] = fmaf(wgt, blend(w0, w1, cv.fu, v1 - v0f), res[m]);
+        res[m] = fmaf(wgt, blend(w0, w1, cv.fu2, v1 - v0f), res[m]);
       }
     } else {
       const float4* e4 = reinterpret_cast<const float4*>(e);
@@ -187,7 +217,7 @@ __device__ __forceinline__ void fast_column(float* __restrict__ vol, const uint3
 #pragma unroll
         for (int i = 0; i < CH; ++i) {
           const float wgt = ok[i] ? rcp_approx(fmaf(qv[i], cv.E, 1.0f)) : 0.0f;
-          res[c * CH + i] = fmaf(wgt, blend(w0[i], w1[i], cv.fu, fz[i]), res[c * CH + i]);
+          res[c * CH + i] = fmaf(wgt, blend(w0[i], w1[i], cv.fu2, fz[i]), res[c * CH + i]);
         }
       }
     }
@@ -198,30 +228,6 @@ __device__ __forceinline__ void fast_column(float* __restrict__ vol, const uint3
     if (z0 + m < P.ZN) out[m] = res[m] * P.DeltaFai;
 }
 
-// ---- packed FP32x2 arithmetic (sm_100: one instruction for two lanes) ----
-__device__ __forceinline__ uint64_t pk2(float a, float b) {
-  uint64_t r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-  return r;
-}
-__device__ __forceinline__ void up2(uint64_t r, float& a, float& b) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
-}
-__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
-  uint64_t d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
-  uint64_t d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
-  uint64_t d;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
 
 // Two slices per instruction: slices (2c, 2c+1) of the thread share packed
 // registers through the row position, the bilinear blend, the weight and the

@@ -814,6 +814,10 @@ def main():
         gups, spv, detail = cpu_baseline(scan)
         line["cpu_baseline"] = {"value": gups, "unit": "GUPS", "cores": detail["cores"], "kind": detail["kind"],
                                 "sample": detail["sample"], "s_per_volume": spv}
+        # beside it, a straight CPU build of the same formulas (the C restatement in oracle/)
+        gups_p, spv_p, detail_p = cpu_baseline(scan, budget_s=10.0, kind="port")
+        line["cpu_port"] = {"value": gups_p, "unit": "GUPS", "cores": detail_p["cores"], "kind": "port",
+                            "sample": detail_p["sample"], "s_per_volume": spv_p}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
