@@ -271,9 +271,11 @@ extern "C" int hr_batch_describe(const hr_batch_plan* p, char* buf, int len) {
   std::vector<float*> vols(p->n, nullptr);
   std::vector<hr::BpFastBatchScan> sc;
   HR_TRY(scans_of(p, vols.data(), &sc));
-  int k = snprintf(buf, (size_t)len, "%d scans, %lld work items in one persistent launch of %d CTAs (>= %d per SM); "
+  int k = snprintf(buf, (size_t)len,
+                   "%d scans, %lld work items in one persistent launch of %d CTAs (>= %d per SM, gathers %s); "
                    "slices per thread by scan:", p->n, hr::bp_fast_batch_items(sc.data(), p->n),
-                   p->ctas[p->variant], hr::kBatchVariants[p->variant].min_ctas);
+                   p->ctas[p->variant], hr::kBatchVariants[p->variant].min_ctas,
+                   hr::kBatchVariants[p->variant].chunk > 0 ? "in chunks of 4 slices" : "per slice");
   for (int i = 0; i < p->n && k > 0 && k < len; ++i) k += snprintf(buf + k, (size_t)(len - k), " %d", p->nz[i]);
   if (k > 0 && k < len)
     k += snprintf(buf + k, (size_t)(len - k), " %s",

@@ -352,8 +352,9 @@ struct BatchParams {
   int* counter;      // zero at launch
 };
 
-// MB: CTAs per SM the register allocation must allow (1: no constraint).
-template <int MB>
+// MB: CTAs per SM the register allocation must allow (1: no constraint);
+// CH: gathers of CH slices issued together (0: one slice at a time).
+template <int MB, int CH>
 __global__ void __launch_bounds__(kBx* kBy, MB) bp_fast_batch_kernel(const __grid_constant__ BatchParams B) {
   __shared__ int s_item;
   const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
@@ -374,11 +375,11 @@ __global__ void __launch_bounds__(kBx* kBy, MB) bp_fast_batch_kernel(const __gri
     const int b = t / S.tiles_y;
     if (xi < S.P.XN && yi < S.P.YN) {
       if (S.nz == 16)
-        column<16, 0>(S.vol, S.fpb, S.T, S.P, xi, yi, b);
+        column<16, CH>(S.vol, S.fpb, S.T, S.P, xi, yi, b);
       else if (S.nz == 8)
-        column<8, 0>(S.vol, S.fpb, S.T, S.P, xi, yi, b);
+        column<8, CH>(S.vol, S.fpb, S.T, S.P, xi, yi, b);
       else
-        column<4, 0>(S.vol, S.fpb, S.T, S.P, xi, yi, b);
+        column<4, CH>(S.vol, S.fpb, S.T, S.P, xi, yi, b);
     }
   }
 }
@@ -612,15 +613,15 @@ long long bp_fast_batch_items(const BpFastBatchScan* scans, int n) {
   return total;
 }
 
-template <int MB>
+template <int MB, int CH>
 static int batch_launch(const BatchParams* B, int* ctas, cudaStream_t s) {
   if (ctas) {
     int per_sm = 0;
-    HR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_fast_batch_kernel<MB>, kBx * kBy, 0));
+    HR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_fast_batch_kernel<MB, CH>, kBx * kBy, 0));
     *ctas = std::max(per_sm, 1) * sm_count();
     return HR_OK;
   }
-  bp_fast_batch_kernel<MB><<<B->grid, dim3(kBx, kBy), 0, s>>>(*B);
+  bp_fast_batch_kernel<MB, CH><<<B->grid, dim3(kBx, kBy), 0, s>>>(*B);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
 }
@@ -628,9 +629,12 @@ static int batch_launch(const BatchParams* B, int* ctas, cudaStream_t s) {
 // ctas != nullptr: report the resident CTAs of batch variant bv; else launch *B.
 static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t s) {
   switch (bv) {
-    case 0: return batch_launch<1>(B, ctas, s);
-    case 1: return batch_launch<10>(B, ctas, s);
-    case 2: return batch_launch<12>(B, ctas, s);
+    case 0: return batch_launch<1, 0>(B, ctas, s);
+    case 1: return batch_launch<10, 0>(B, ctas, s);
+    case 2: return batch_launch<12, 0>(B, ctas, s);
+    case 3: return batch_launch<1, 4>(B, ctas, s);
+    case 4: return batch_launch<10, 4>(B, ctas, s);
+    case 5: return batch_launch<12, 4>(B, ctas, s);
     default: return hr::fail(HR_ERR_INVALID_ARGUMENT, "batch backprojection: unknown variant %d", bv);
   }
 }

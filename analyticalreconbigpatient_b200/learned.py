@@ -141,7 +141,8 @@ def pair_scans(grid: int = 512, pixel: float = 0.9766, slices: int = 20, rotatio
 class PairSet:
     """Half-view input volumes and full-view target slices of seeded phantoms,
     resident on the device: inputs [n][YN][XN][ZN] FP32, targets [n][S][YN][XN]
-    FP32 for the S = ZN - 4 slices with a full 5-slice context."""
+    FP32 for the S = ZN - 4 slices with a full 5-slice context. I0: photons per
+    ray of the Poisson noise added before the log (0: noiseless data)."""
 
     def __init__(self, seeds, grid: int = 512, pixel: float = 0.9766, slices: int = 20, I0: float = 1e5,
                  n_ellipsoids: int = 60, device: int = 0):
@@ -165,7 +166,8 @@ class PairSet:
             objs = P.random_ellipsoids(seed, n_ellipsoids, (zlo, zhi), body=(180.0 * scale, 140.0 * scale),
                                        semi_axes=(5.0 * scale, 120.0 * scale))
             fan = project(f, objs, device=self.device.index)
-            add_poisson_noise(fan, I0, 0x5EED0000 + seed)
+            if I0 > 0:
+                add_poisson_noise(fan, I0, 0x5EED0000 + seed)
             rf.run(fan, vol_f)
             half_fan = fan[::2].contiguous()
             rh.run(half_fan, self.inputs[k])
@@ -247,18 +249,19 @@ def main(argv=None) -> None:
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--grid", type=int, default=512)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--i0", type=float, default=1e5, help="photons per ray before the log (0: noiseless)")
     ap.add_argument("--save", default=None, help="write the trained parameters (.npy)")
     a = ap.parse_args(argv)
     pixel = 0.9766 * 512 / a.grid
     t0 = time.perf_counter()
-    train_set = PairSet(range(1, 1 + a.phantoms), grid=a.grid, pixel=pixel)
+    train_set = PairSet(range(1, 1 + a.phantoms), grid=a.grid, pixel=pixel, I0=a.i0)
     t1 = time.perf_counter()
     net = Corrector(seed=a.seed)
     losses = train(net, train_set, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     del train_set
-    test_set = PairSet(range(100001, 100001 + a.eval), grid=a.grid, pixel=pixel)
+    test_set = PairSet(range(100001, 100001 + a.eval), grid=a.grid, pixel=pixel, I0=a.i0)
     ev = evaluate(net, test_set)
     if a.save:
         np.save(a.save, net.params())

@@ -448,6 +448,8 @@ def run_bigpatient(args, scan, dev, world, rank, barrier):
                     "h2d_bytes_per_step": scan.projection_bytes(), "d2h_bytes_per_step": scan.volume_bytes(),
                     "host_memory": "pinned" if pinned else "pageable",
                     "entry": "hr_slab_execute (C ABI, host buffers)"},
+            # per slab: rebin, split, Toeplitz GEMM, backprojection
+            "gpu_launches": 4 * ((scan.ZN + args.slab - 1) // args.slab) * args.steps,
             "kernels": desc, "clocks": clocks.summary()}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -55,7 +55,7 @@ def solo(scan, fan, fast_variant):
 NZ_TO_FAST = {16: 0, 8: 3, 4: 8}
 
 
-@pytest.mark.parametrize("bv", [0, 1, 2])
+@pytest.mark.parametrize("bv", [0, 1, 2, 3, 5])
 def test_batch_equals_each_scan_alone(cuda, bv):
     scans = uneven_scans()
     fans = fans_for(scans, noise=True)
@@ -103,7 +103,7 @@ def test_batch_graph_replay_and_new_buffers(cuda):
 def test_batch_autotuner_reports_every_variant(cuda):
     rec = BatchRecon(uneven_scans()[:2])
     desc = rec.describe()
-    assert "autotuned" in desc and all(f"v{v}=" in desc for v in range(3)), desc
+    assert "autotuned" in desc and all(f"v{v}=" in desc for v in range(6)), desc
     rec.close()
 
 
