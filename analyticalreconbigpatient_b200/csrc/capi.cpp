@@ -132,7 +132,8 @@ extern "C" int hr_bp_host_double(double* hctimage, const double* hfp, const doub
                                  double BetaS, double DeltaFai, double N_pi, double HSCoef, double SO, double SD,
                                  double k1) {
   hr::clear_error();
-  HR_REQUIRE(hctimage != nullptr && hfp != nullptr && hw != nullptr, "ParallekFDKHelical3DWeighting_GPU_double: NULL pointer");
+  HR_REQUIRE(hctimage != nullptr && hfp != nullptr && hw != nullptr,
+             "ParallekFDKHelical3DWeighting_GPU_double: NULL pointer");
   const hr_bp_geom g = make_geom(N_2pi, XN, YN, ZN, XNC, YNC, ZNC, dx, dy, dz, YL, ZL, PN, YLC, ZLC, dYL, dZL, h,
                                  BetaS, DeltaFai, N_pi, HSCoef, SO, SD, k1);
   return bp_host(hctimage, sizeof(double), hfp, sizeof(double), g, hw, HR_FORM_FP64);

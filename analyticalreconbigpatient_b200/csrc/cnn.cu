@@ -184,6 +184,66 @@ struct ConvArgs {
   int* err;
 };
 
+// Epilogue of one output row segment: the thread's pixel (b, y, x) with its COUT accumulator values.
+template <int COUT, int EPI>
+__device__ __forceinline__ void conv_epilogue(const ConvArgs& a, const float (&v)[COUT], const float* bias_s, int b,
+                                              int y, int x, int lane) {
+  const bool valid = x < a.W;
+  const size_t pix = ((size_t)b * a.H + y) * a.W + x;
+  if constexpr (EPI == EPI_RELU) {
+    if (valid) {
+      uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
+#pragma unroll
+      for (int c = 0; c < COUT / 8; ++c) {
+        float u[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) u[j] = fmaxf(v[8 * c + j] + bias_s[8 * c + j], 0.0f);
+        o[c] = make_uint4(pack2(u[0], u[1]), pack2(u[2], u[3]), pack2(u[4], u[5]), pack2(u[6], u[7]));
+      }
+    }
+  } else if constexpr (EPI == EPI_MASK) {
+    if (valid) {
+      const uint4* m = reinterpret_cast<const uint4*>(a.mask + pix * COUT);
+      uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
+#pragma unroll
+      for (int c = 0; c < COUT / 8; ++c) {
+        const uint4 mv = __ldg(m + c);
+        const uint32_t mw[4] = {mv.x, mv.y, mv.z, mv.w};
+        float u[8];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          u[2 * j] = bf_lo(mw[j]) > 0.0f ? v[8 * c + 2 * j] : 0.0f;
+          u[2 * j + 1] = bf_hi(mw[j]) > 0.0f ? v[8 * c + 2 * j + 1] : 0.0f;
+        }
+        o[c] = make_uint4(pack2(u[0], u[1]), pack2(u[2], u[3]), pack2(u[4], u[5]), pack2(u[6], u[7]));
+      }
+    }
+  } else {
+    const float r = v[0] + bias_s[0];
+    float e2 = 0.0f;
+    if (valid) {
+      const size_t off = (size_t)b * a.sb + ((size_t)y * a.W + x) * a.sp;
+      const float pr = a.base[off] + a.scale * r;
+      if constexpr (EPI == EPI_RESID) {
+        a.pred[off] = pr;
+      } else {
+        if (a.pred) a.pred[off] = pr;
+        const float e = (pr - a.target[off]) / a.scale;
+        e2 = e * e;
+        uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
+        o[0] = make_uint4(pack2(a.grad_scale * e, 0.0f), 0u, 0u, 0u);
+#pragma unroll
+        for (int c = 1; c < COUT / 8; ++c) o[c] = make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+    if constexpr (EPI == EPI_LOSS) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+      if (lane == 0 && e2 != 0.0f) atomicAdd(a.loss, e2);
+    }
+  }
+}
+
 template <int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant__ ConvArgs a) {
   constexpr int G = CIN / 8;                 // 8-channel groups (TMA boxes per input row)
@@ -244,7 +304,8 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
       int h = 0;  // input rows loaded by this CTA
       bool ok = true;
       for (long long un = blockIdx.x; un < units && ok; un += gridDim.x) {
-        const int seg = (int)(un % nseg), chunk = (int)((un / nseg) % nchunk), b = (int)(un / ((long long)nseg * nchunk));
+        const int seg = (int)(un % nseg), chunk = (int)((un / nseg) % nchunk);
+        const int b = (int)(un / ((long long)nseg * nchunk));
         const int y0 = chunk * rpu, ny = min(rpu, a.H - y0);
         for (int j = 0; j < ny + 2; ++j, ++h) {
           const int s = h % kRing;
@@ -301,76 +362,22 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
     int it = 0;
     bool ok = true;
     for (long long un = blockIdx.x; un < units && ok; un += gridDim.x) {
-     const int seg = (int)(un % nseg), chunk = (int)((un / nseg) % nchunk), b = (int)(un / ((long long)nseg * nchunk));
-     const int y0 = chunk * rpu, ny = min(rpu, a.H - y0);
-     for (int i = 0; i < ny; ++i, ++it) {
-      const int acc = it & 1;
-      if (!mbar_wait(&tfull[acc], (it >> 1) & 1, abort_flag, a.err)) {
-        ok = false;
-        break;
+      const int seg = (int)(un % nseg), chunk = (int)((un / nseg) % nchunk);
+      const int b = (int)(un / ((long long)nseg * nchunk));
+      const int y0 = chunk * rpu, ny = min(rpu, a.H - y0);
+      for (int i = 0; i < ny; ++i, ++it) {
+        const int acc = it & 1;
+        if (!mbar_wait(&tfull[acc], (it >> 1) & 1, abort_flag, a.err)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        float v[COUT];
+        tmem_ld<COUT>(tmem + acc * 32 + ((uint32_t)(q * 32) << 16), v);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive(&tempty[acc]);  // the registers hold the tile: the accumulator may be reused
+        conv_epilogue<COUT, EPI>(a, v, bias_s, b, y0 + i, seg * kTileM + q * 32 + lane, lane);
       }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      float v[COUT];
-      tmem_ld<COUT>(tmem + acc * 32 + ((uint32_t)(q * 32) << 16), v);
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      mbar_arrive(&tempty[acc]);  // the registers hold the tile: the accumulator may be reused
-      const int y = y0 + i;
-      const int x = seg * kTileM + q * 32 + lane;
-      const bool valid = x < a.W;
-      const size_t pix = ((size_t)b * a.H + y) * a.W + x;
-      if constexpr (EPI == EPI_RELU) {
-        if (valid) {
-          uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
-#pragma unroll
-          for (int c = 0; c < COUT / 8; ++c) {
-            float u[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) u[j] = fmaxf(v[8 * c + j] + bias_s[8 * c + j], 0.0f);
-            o[c] = make_uint4(pack2(u[0], u[1]), pack2(u[2], u[3]), pack2(u[4], u[5]), pack2(u[6], u[7]));
-          }
-        }
-      } else if constexpr (EPI == EPI_MASK) {
-        if (valid) {
-          const uint4* m = reinterpret_cast<const uint4*>(a.mask + pix * COUT);
-          uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
-#pragma unroll
-          for (int c = 0; c < COUT / 8; ++c) {
-            const uint4 mv = __ldg(m + c);
-            const uint32_t mw[4] = {mv.x, mv.y, mv.z, mv.w};
-            float u[8];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              u[2 * j] = bf_lo(mw[j]) > 0.0f ? v[8 * c + 2 * j] : 0.0f;
-              u[2 * j + 1] = bf_hi(mw[j]) > 0.0f ? v[8 * c + 2 * j + 1] : 0.0f;
-            }
-            o[c] = make_uint4(pack2(u[0], u[1]), pack2(u[2], u[3]), pack2(u[4], u[5]), pack2(u[6], u[7]));
-          }
-        }
-      } else {
-        const float r = v[0] + bias_s[0];
-        float e2 = 0.0f;
-        if (valid) {
-          const size_t off = (size_t)b * a.sb + ((size_t)y * a.W + x) * a.sp;
-          const float pr = a.base[off] + a.scale * r;
-          if constexpr (EPI == EPI_RESID) {
-            a.pred[off] = pr;
-          } else {
-            if (a.pred) a.pred[off] = pr;
-            const float e = (pr - a.target[off]) / a.scale;
-            e2 = e * e;
-            uint4* o = reinterpret_cast<uint4*>(a.out + pix * COUT);
-            o[0] = make_uint4(pack2(a.grad_scale * e, 0.0f), 0u, 0u, 0u);
-#pragma unroll
-            for (int c = 1; c < COUT / 8; ++c) o[c] = make_uint4(0u, 0u, 0u, 0u);
-          }
-        }
-        if constexpr (EPI == EPI_LOSS) {
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
-          if (lane == 0 && e2 != 0.0f) atomicAdd(a.loss, e2);
-        }
-      }
-     }
     }
   }
   __syncthreads();

@@ -260,7 +260,8 @@ extern "C" int hr_filter_plan_create(hr_filter_plan** plan, int YL, int ZL, int 
     H[k] = (float)(acc / N);
   }
   std::vector<float2> tw(N);
-  for (int t = 0; t < N; ++t) tw[t] = make_float2((float)std::cos(2.0 * M_PI * t / N), (float)-std::sin(2.0 * M_PI * t / N));
+  for (int t = 0; t < N; ++t)
+    tw[t] = make_float2((float)std::cos(2.0 * M_PI * t / N), (float)-std::sin(2.0 * M_PI * t / N));
   hr_filter_plan* p = new hr_filter_plan{YL, ZL, ViewN, log2N, PLC, ZLC, dYL, dZL, SO, nullptr, nullptr};
   cudaError_t e = cudaMalloc(&p->d_H, sizeof(float) * N);
   if (e == cudaSuccess) e = cudaMalloc(&p->d_tw, sizeof(float2) * N);

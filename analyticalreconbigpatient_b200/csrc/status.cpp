@@ -23,7 +23,8 @@ int require_device() {
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0) {
     cudaGetLastError();
-    return fail(HR_ERR_NO_DEVICE, "no CUDA device available (%s)", e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+    return fail(HR_ERR_NO_DEVICE, "no CUDA device available (%s)",
+                e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
   }
   return HR_OK;
 }
