@@ -12,6 +12,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libhelixrecon.so")
 
 HR_OK = 0
+HR_ERR_INVALID_ARGUMENT, HR_ERR_CUDA, HR_ERR_OUT_OF_MEMORY, HR_ERR_NO_DEVICE, HR_ERR_UNSUPPORTED = 1, 2, 3, 4, 5
 HR_FORM_PLAIN, HR_FORM_FP64, HR_FORM_FAST = 0, 1, 2
 HR_LAYOUT_ROWS, HR_LAYOUT_REBIN = 0, 1
 

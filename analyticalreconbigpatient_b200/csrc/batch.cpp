@@ -210,6 +210,11 @@ extern "C" int hr_batch_plan_create(hr_batch_plan** plan, const hr_recon_desc* d
     destroy(p);
     return st;
   }
+  if (hr::log_enabled()) {
+    char desc[768];
+    if (hr_batch_describe(p, desc, sizeof(desc)) == HR_OK)
+      hr::log("batch plan: %.2f GB on the device; %s", hr_batch_device_bytes(p) / 1e9, desc);
+  }
   *plan = p;
   return HR_OK;
 }

@@ -36,7 +36,7 @@
 
 namespace {
 
-constexpr int kBx = 8, kBy = 16;  // CTA tile (x, y): 4 warps of 8 x 4 columns
+constexpr int kBx = 8, kBy = 32;  // CTA tile (x, y): 8 warps of 8 x 4 columns
 constexpr double kTwoPiTrunc = 2.0 * 3.14159265358979;
 constexpr double kInvTwoPi = 1.0 / (2.0 * 3.141592653589793);
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: adding it rounds to an integer
@@ -630,11 +630,11 @@ static int batch_launch(const BatchParams* B, int* ctas, cudaStream_t s) {
 static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t s) {
   switch (bv) {
     case 0: return batch_launch<1, 0>(B, ctas, s);
-    case 1: return batch_launch<10, 0>(B, ctas, s);
-    case 2: return batch_launch<12, 0>(B, ctas, s);
+    case 1: return batch_launch<5, 0>(B, ctas, s);
+    case 2: return batch_launch<6, 0>(B, ctas, s);
     case 3: return batch_launch<1, 4>(B, ctas, s);
-    case 4: return batch_launch<10, 4>(B, ctas, s);
-    case 5: return batch_launch<12, 4>(B, ctas, s);
+    case 4: return batch_launch<5, 4>(B, ctas, s);
+    case 5: return batch_launch<6, 4>(B, ctas, s);
     default: return hr::fail(HR_ERR_INVALID_ARGUMENT, "batch backprojection: unknown variant %d", bv);
   }
 }
@@ -752,9 +752,9 @@ int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t*
 int bp_fast_describe(const BpFast& f, char* buf, int len) {
   if (!buf || len <= 0) return HR_OK;
   const FastVariant& fv = kFastVariants[f.variant];
-  int n = snprintf(buf, (size_t)len, "slices_per_thread=%d gathers=%s tile=8x16 %s", kFastNz[fv.table],
+  int n = snprintf(buf, (size_t)len, "slices_per_thread=%d gathers=%s tile=%dx%d %s", kFastNz[fv.table],
                    fv.chunk < 0 ? "paired-f32x2" : fv.chunk == 0 ? "per-slice" : fv.chunk == 4 ? "chunk4" : "chunk8",
-                   f.tuned == 2 ? "(pinned by HELIXRECON_BP_VARIANT)"
+                   kBx, kBy, f.tuned == 2 ? "(pinned by HELIXRECON_BP_VARIANT)"
                    : f.tuned ? "(autotuned; ms/slice:" : "(default)");
   if (f.tuned == 1) {
     for (int v = 0; v < kFastVariants_n && n > 0 && n < len; ++v)

@@ -84,12 +84,12 @@ int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t*
 int bp_fast_describe(const BpFast& f, char* buf, int len);
 // Several scans in one persistent launch. Each scan runs the kernel body with
 // its own slices per thread (16, 8 or 4); batch variants differ in the CTAs
-// per SM their registers must allow (1: unconstrained; 10; 12) and in the
+// (of 256 threads) per SM their registers must allow (1: unconstrained; 5; 6) and in the
 // gathers issued together (one slice at a time, or chunks of 4 slices).
 struct BatchVariant {
   int min_ctas, chunk;
 };
-constexpr BatchVariant kBatchVariants[] = {{1, 0}, {10, 0}, {12, 0}, {1, 4}, {10, 4}, {12, 4}};
+constexpr BatchVariant kBatchVariants[] = {{1, 0}, {5, 0}, {6, 0}, {1, 4}, {5, 4}, {6, 4}};
 constexpr int kBatchVariants_n = sizeof(kBatchVariants) / sizeof(kBatchVariants[0]);
 struct BpFastBatchScan {
   const BpFast* f;

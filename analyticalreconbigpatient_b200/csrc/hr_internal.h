@@ -15,6 +15,9 @@ namespace hr {
 // returns `code`, so that call sites can `return fail(...)`.
 int fail(int code, const char* fmt, ...);
 void clear_error();
+// Diagnostic line on stderr when the environment variable HELIXRECON_LOG is set (and not "0").
+bool log_enabled();
+void log(const char* fmt, ...);
 
 // Checks a CUDA runtime call; on failure records file:line and the CUDA
 // message and returns HR_ERR_CUDA (HR_ERR_OUT_OF_MEMORY for allocation).

@@ -96,6 +96,12 @@ extern "C" int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* d
     destroy(p);
     return st;
   }
+  if (hr::log_enabled()) {
+    char desc[512];
+    if (hr_recon_describe(p, desc, sizeof(desc)) == HR_OK)
+      hr::log("recon plan: %d views -> %dx%dx%d, %.2f GB on the device; %s", d->ViewN, d->bp.XN, d->bp.YN, d->bp.ZN,
+              hr_recon_device_bytes(p) / 1e9, desc);
+  }
   *plan = p;
   return HR_OK;
 }

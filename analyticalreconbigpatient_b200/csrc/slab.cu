@@ -223,6 +223,10 @@ static int prepare(hr_slab_plan* p, const float* fan, bool fan_on_host) {
     cudaGraphDestroy(gr);
     HR_CUDA_TRY(ei);
   }
+  if (hr::log_enabled()) {
+    char desc[768];
+    if (hr_slab_describe(p, desc, sizeof(desc)) == HR_OK) hr::log("slab plan prepared: %s", desc);
+  }
   return HR_OK;
 }
 

@@ -1,4 +1,5 @@
 // Error reporting and device helpers.
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -9,6 +10,9 @@ namespace hr {
 static thread_local char g_last_error[1024] = {0};
 
 int fail(int code, const char* fmt, ...) {
+  // a failed runtime call (an allocation, a launch configuration) leaves its error as the thread's
+  // last CUDA error; clear it so that it is not reported again by the caller's next CUDA call
+  if (code == HR_ERR_CUDA || code == HR_ERR_OUT_OF_MEMORY) cudaGetLastError();
   va_list ap;
   va_start(ap, fmt);
   vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
@@ -17,6 +21,25 @@ int fail(int code, const char* fmt, ...) {
 }
 
 void clear_error() { g_last_error[0] = 0; }
+
+// HELIXRECON_LOG=1 prints the plans' configuration choices to stderr.
+bool log_enabled() {
+  static const int on = [] {
+    const char* e = std::getenv("HELIXRECON_LOG");
+    return (e && *e && std::strcmp(e, "0") != 0) ? 1 : 0;
+  }();
+  return on != 0;
+}
+
+void log(const char* fmt, ...) {
+  if (!log_enabled()) return;
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  std::fprintf(stderr, "[helixrecon] %s\n", buf);
+}
 
 int require_device() {
   int n = 0;

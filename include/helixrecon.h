@@ -284,8 +284,9 @@ int hr_batch_execute(hr_batch_plan* plan, float* const* d_vols, const float* con
  * hr_batch_execute left in the plan (not captured; for timing the kernel). */
 int hr_batch_backproject(hr_batch_plan* plan, float* const* d_vols, void* stream);
 /* Selects a batch backprojection variant (0..5: registers unconstrained, or
- * limited for 10 or 12 CTAs per SM; gathers per slice (0..2) or in chunks of 4
- * slices (3..5)); each scan keeps the slices per thread its own autotuner chose. */
+ * limited for 5 or 6 CTAs of 256 threads per SM; gathers per slice (0..2) or in
+ * chunks of 4 slices (3..5)); each scan keeps the slices per thread its own
+ * autotuner chose. */
 int hr_batch_select(hr_batch_plan* plan, int variant);
 int hr_batch_describe(const hr_batch_plan* plan, char* buf, int len);
 int hr_batch_check(const hr_batch_plan* plan);

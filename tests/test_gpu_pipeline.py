@@ -7,6 +7,8 @@ FP64, the double backprojection (bit-identical to
 ParallelFDKHelical3DWeightingCPU). "FP64 oracle" = the same chain with an FP64
 rebinning.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -96,3 +98,37 @@ def test_offcentre_sphere_lands_at_its_position(cuda):
     m = np.where(d > 0.5 * d.max(), d, 0.0)
     c = [(m * a).sum() / m.sum() for a in (x, y, z)]
     assert abs(c[0] - cx) < 0.5 * sc.dx and abs(c[1] - cy) < 0.5 * sc.dy and abs(c[2] - cz) < 0.5 * sc.dz, c
+
+
+def test_out_of_memory_is_reported_and_the_device_stays_usable(cuda):
+    import torch
+    from analyticalreconbigpatient_b200.pipeline import HelicalRecon
+
+    # 1200 rotations of the 888 x 64 detector: the rebinned buffer alone would take 268 GB
+    huge = G.Scan(ZL=64, pitch=0.984, rotations=1200, XN=64, YN=64, ZN=4, dx=4.0, dy=4.0, dz=1.0)
+    with pytest.raises(_lib.HelixError) as exc:
+        HelicalRecon(huge, form=_lib.HR_FORM_PLAIN)
+    assert exc.value.status == _lib.HR_ERR_OUT_OF_MEMORY, exc.value
+    sc = G.tiny()
+    rec = HelicalRecon(sc)
+    fan = torch.zeros((sc.views, sc.YL, sc.ZL), device=cuda)
+    vol = rec.run(fan)
+    torch.cuda.synchronize()
+    assert float(vol.abs().max()) == 0.0
+    rec.close()
+
+
+def test_log_variable_prints_plan_choices(cuda):
+    import subprocess
+    import sys
+
+    code = ("from analyticalreconbigpatient_b200 import _lib, geometry as G\n"
+            "from analyticalreconbigpatient_b200.pipeline import HelicalRecon\n"
+            "HelicalRecon(G.tiny(YL=200, ZL=8), form=_lib.HR_FORM_FAST).close()\n")
+    env = dict(os.environ, HELIXRECON_LOG="1")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "[helixrecon] recon plan:" in r.stderr and "autotuned" in r.stderr, r.stderr
+    env["HELIXRECON_LOG"] = "0"
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert "[helixrecon]" not in r.stderr
