@@ -108,12 +108,15 @@ def test_pack_pairs_layout(cuda):
     assert np.all(hi[:, -1] == 0)
 
 
-def test_every_fast_variant_gives_the_same_volume(cuda):
+@pytest.mark.parametrize("pixel", [5.0, 0.9766])
+def test_every_fast_variant_gives_the_same_volume(cuda, pixel):
     """The autotuner's candidates differ only in work distribution: the same
-    FP32 operations per (voxel, view) in the same view order, so identical bits."""
+    FP32 operations per (voxel, view) in the same view order, so identical bits.
+    Coarse 5 mm voxels spread a CTA's taps over the whole detector; 0.98 mm
+    voxels (the clinical 500 mm / 512 grid) keep them within a few channels."""
     from analyticalreconbigpatient_b200.pipeline import StagePlans
 
-    sc = G.Scan(ZL=16, pitch=0.9375, rotations=3, XN=40, YN=48, ZN=37, dx=5.0, dy=5.0, dz=1.0)
+    sc = G.Scan(ZL=16, pitch=0.9375, rotations=3, XN=40, YN=48, ZN=37, dx=pixel, dy=pixel, dz=1.0)
     rng = np.random.default_rng(3)
     filt = torch.tensor(rng.standard_normal((sc.PN, sc.ZL, sc.YL)).astype(np.float32), device=cuda)
     fast = StagePlans(sc, _lib.HR_FORM_FAST)
