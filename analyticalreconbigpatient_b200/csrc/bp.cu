@@ -377,7 +377,7 @@ extern "C" int hr_bp_select(hr_bp_plan* pl, int variant) {
   HR_REQUIRE(variant >= 0 && variant < hr::kFastVariants_n, "hr_bp_select: variant %d out of range [0, %d)",
              variant, hr::kFastVariants_n);
   pl->fast.variant = variant;
-  return HR_OK;
+  return hr::bp_fast_tex_prepare(&pl->fast, pl->fg);
 }
 
 extern "C" int hr_bp_describe(const hr_bp_plan* pl, char* buf, int len) {

@@ -25,6 +25,7 @@
 // reference's ceil; both give the same interpolated value away from exact
 // integers, where the blend is continuous.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
@@ -384,6 +385,123 @@ __global__ void __launch_bounds__(kBx* kBy, MB) bp_fast_batch_kernel(const __gri
   }
 }
 
+// ---- texture variants ----
+// The filtered data as layered 2D textures (one layer per view), sampled with
+// the texture units' bilinear filtering at (u1 + 1/2, V + 1/2): one TEX per
+// update replaces the two gathers, the BF16 unpacking and the three blends.
+// The hardware blends with 1.8 fixed-point weights, so a tap differs from the
+// FP32 blend by up to 1/256 of the neighbour difference (the fast form's
+// accuracy budget covers it). Taps come from the low halves of the BF16 pairs:
+// the same sample values as the gather variants (FP16 holds every BF16 value
+// of the scaled range exactly).
+
+// Largest |value| of the filtered data (bits of a non-negative float order
+// like unsigned integers), for the FP16 scale.
+__global__ void tex_absmax_kernel(float* __restrict__ scale, const uint32_t* __restrict__ fpb, long long n) {
+  unsigned m = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = max(m, (__ldg(fpb + i) << 16) & 0x7fffffffu);
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(reinterpret_cast<unsigned*>(scale + 1), m);
+}
+
+// BF16 pairs [views][ZL][YL] -> the layered arrays. FP16: scaled by 2^k with
+// the largest |value| below 2^15; scale[0] = 2^-k, which the backprojection
+// folds into its output. One CTA row at a time (rows = views x ZL).
+template <bool HALF>
+__global__ void tex_fill_kernel(float* __restrict__ scale, const unsigned long long* __restrict__ surfs,
+                                const uint32_t* __restrict__ fpb, long long rows, int ZL, int YL, int lsh) {
+  float sc = 1.0f;
+  if constexpr (HALF) {
+    const int e = (int)(__float_as_uint(scale[1]) >> 23) - 127;  // max |value| < 2^(e+1)
+    const int k = min(max(127 + 14 - e, 1), 253);                  // biased exponent of 2^(14-e)
+    sc = __int_as_float(k << 23);
+    if (blockIdx.x == 0 && threadIdx.x == 0) scale[0] = __int_as_float((254 - k) << 23);
+  } else {
+    if (blockIdx.x == 0 && threadIdx.x == 0) scale[0] = 1.0f;
+  }
+  const int lmask = (1 << lsh) - 1;
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int p = (int)(r / ZL), v = (int)(r - (long long)p * ZL);
+    const cudaSurfaceObject_t so = surfs[p >> lsh];
+    const uint32_t* row = fpb + r * YL;
+    for (int u = threadIdx.x; u < YL; u += blockDim.x) {
+      const float val = __uint_as_float(__ldg(row + u) << 16);
+      if constexpr (HALF)
+        surf2DLayeredwrite(__half_as_ushort(__float2half_rn(val * sc)), so, u * 2, v, p & lmask, cudaBoundaryModeZero);
+      else
+        surf2DLayeredwrite(val, so, u * 4, v, p & lmask, cudaBoundaryModeZero);
+    }
+  }
+}
+
+// Same tables, window masks and weight as fast_column; the tap is a texture
+// sample. The NZ samples of a (column, view) are issued before any is used.
+template <int NZ>
+__global__ void __launch_bounds__(kBx* kBy) bp_tex_kernel(float* __restrict__ vol,
+                                                         const unsigned long long* __restrict__ texs, int lsh,
+                                                         const float* __restrict__ scale, const ZTabs T,
+                                                         const FastParams P, int b_first) {
+  static_assert(NZ % 2 == 0, "table entries are read two slices at a time");
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  if (xi >= P.XN || yi >= P.YN) return;
+  const int b = b_first + blockIdx.z;
+  const int z0 = b * NZ;
+  const int2 blk = T.zblock[b];
+  const int off = T.zoff[b];
+  const float x = ((float)xi - P.XNC) * P.dx;
+  const float y = ((float)yi - P.YNC) * P.dy;
+  float res[NZ];
+#pragma unroll
+  for (int m = 0; m < NZ; ++m) res[m] = 0.0f;
+  const float4* btab = reinterpret_cast<const float4*>(T.ztab + (size_t)off * NZ);
+  const uint32_t* bmask = T.zmask + off;
+  const float utop = (float)(P.YL - 1), vtop = (float)P.ZL - 0.5f;
+  const float zlch = P.ZLC0 + 0.5f;
+  const int lmask = (1 << lsh) - 1;
+  for (int q = 0; q < blk.y; ++q) {
+    const uint32_t mask = __ldg(bmask + q);
+    if (mask == 0u) continue;
+    const int p = blk.x + q;
+    const float2 cs = __ldg(T.trig + p);
+    const float UU = -x * cs.x - y * cs.y;
+    const float Yr = -x * cs.y + y * cs.x;
+    const float u1 = fmaf(Yr, P.invdYL, P.YLC0);
+    if (!(u1 >= 0.0f && u1 < utop)) continue;  // floor(u1) in [0, YL-2]
+    const float t1sq = P.SO2 - Yr * Yr;
+    const float temp1 = t1sq * rsqrtf(t1sq);
+    const float A = temp1 + UU, B = temp1 - UU;
+    const float K = P.SOSDdZL * rcp_approx(temp1 * A);
+    const float E = ex2_approx(P.k1 * lg2_approx(B * rcp_approx(A)));
+    const cudaTextureObject_t tx = __ldg(texs + (p >> lsh));
+    const int layer = p & lmask;
+    const float xt = u1 + 0.5f;
+    const float4* e = btab + (size_t)q * (NZ / 2);
+    float tap[NZ], qv[NZ];
+#pragma unroll
+    for (int c = 0; c < NZ / 2; ++c) {
+      const float4 t = __ldg(e + c);  // {t2, 2^Q} of slices 2c and 2c+1
+      qv[2 * c] = t.y;
+      qv[2 * c + 1] = t.w;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int m = 2 * c + i;
+        const float vh = fmaf(i ? t.z : t.x, K, zlch);  // row position + 1/2
+        const bool ok = ((mask >> m) & 1u) && vh >= 0.5f && vh < vtop;  // floor in [0, ZL-2]
+        tap[m] = ok ? tex2DLayered<float>(tx, xt, vh, layer) : 0.0f;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < NZ; ++m) res[m] = fmaf(rcp_approx(fmaf(qv[m], E, 1.0f)), tap[m], res[m]);
+  }
+  const float outs = P.DeltaFai * __ldg(scale);
+  float* out = vol + ((size_t)yi * P.XN + xi) * P.ZN + z0;
+#pragma unroll
+  for (int m = 0; m < NZ; ++m)
+    if (z0 + m < P.ZN) out[m] = res[m] * outs;
+}
+
 // fp32 [n][YL] rows -> BF16 pairs (u, u+1), round to nearest even.
 __global__ void pack_pairs_kernel(uint32_t* __restrict__ out, const float* __restrict__ in, long long rows, int YL) {
   const long long total = rows * YL;
@@ -534,7 +652,102 @@ int bp_fast_create(BpFast* f, const BpFastGeom& g, const double* w) {
   return HR_OK;
 }
 
+static void tex_free(BpFastTex* t) {
+  for (unsigned long long o : t->tex) cudaDestroyTextureObject(o);
+  for (unsigned long long o : t->surf) cudaDestroySurfaceObject(o);
+  for (cudaArray_t a : t->arr) cudaFreeArray(a);
+  cudaFree(t->d_obj);
+  cudaFree(t->d_scale);
+  *t = BpFastTex{};
+}
+
+static int tex_alloc_arrays(BpFastTex* t, int kind, int YL, int ZL, int views) {
+  int dev = 0, mw = 0, mh = 0, ml = 0;
+  HR_CUDA_TRY(cudaGetDevice(&dev));
+  HR_CUDA_TRY(cudaDeviceGetAttribute(&mw, cudaDevAttrMaxSurface2DLayeredWidth, dev));
+  HR_CUDA_TRY(cudaDeviceGetAttribute(&mh, cudaDevAttrMaxSurface2DLayeredHeight, dev));
+  HR_CUDA_TRY(cudaDeviceGetAttribute(&ml, cudaDevAttrMaxSurface2DLayeredLayers, dev));
+  int tw = 0, th = 0, tl = 0;
+  HR_CUDA_TRY(cudaDeviceGetAttribute(&tw, cudaDevAttrMaxTexture2DLayeredWidth, dev));
+  HR_CUDA_TRY(cudaDeviceGetAttribute(&th, cudaDevAttrMaxTexture2DLayeredHeight, dev));
+  HR_CUDA_TRY(cudaDeviceGetAttribute(&tl, cudaDevAttrMaxTexture2DLayeredLayers, dev));
+  const int esz = kind == kTexHalf ? 2 : 4;
+  HR_REQUIRE(YL * esz <= mw && YL <= tw && ZL <= std::min(mh, th) && std::min(ml, tl) >= 2,
+             "fast backprojection: %d x %d detector rows exceed the layered texture limits", ZL, YL);
+  t->kind = kind;
+  t->YL = YL;
+  t->ZL = ZL;
+  t->views = views;
+  t->lsh = 0;
+  while ((2 << t->lsh) <= std::min(std::min(ml, tl), 2048)) ++t->lsh;
+  const int L = 1 << t->lsh;
+  t->n = (views + L - 1) / L;
+  const cudaChannelFormatDesc desc = kind == kTexHalf ? cudaCreateChannelDescHalf() : cudaCreateChannelDesc<float>();
+  for (int i = 0; i < t->n; ++i) {
+    const int layers = std::min(L, views - i * L);
+    cudaArray_t a = nullptr;
+    HR_CUDA_TRY(cudaMalloc3DArray(&a, &desc, make_cudaExtent(YL, ZL, layers),
+                                  cudaArrayLayered | cudaArraySurfaceLoadStore));
+    t->arr.push_back(a);
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = a;
+    cudaTextureDesc td{};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaTextureObject_t to = 0;
+    HR_CUDA_TRY(cudaCreateTextureObject(&to, &rd, &td, nullptr));
+    t->tex.push_back(to);
+    cudaSurfaceObject_t so = 0;
+    HR_CUDA_TRY(cudaCreateSurfaceObject(&so, &rd));
+    t->surf.push_back(so);
+  }
+  std::vector<unsigned long long> obj(t->tex);
+  obj.insert(obj.end(), t->surf.begin(), t->surf.end());
+  HR_CUDA_TRY(cudaMalloc(&t->d_obj, sizeof(unsigned long long) * obj.size()));
+  HR_CUDA_TRY(cudaMemcpy(t->d_obj, obj.data(), sizeof(unsigned long long) * obj.size(), cudaMemcpyHostToDevice));
+  HR_CUDA_TRY(cudaMalloc(&t->d_scale, 2 * sizeof(float)));
+  t->bytes = (size_t)views * YL * ZL * esz;
+  return HR_OK;
+}
+
+// Arrays of the given kind for `views` views (kept when they already fit).
+static int tex_alloc(BpFastTex* t, int kind, int YL, int ZL, int views) {
+  if (t->kind == kind && (kind == 0 || (t->YL == YL && t->ZL == ZL && t->views >= views))) return HR_OK;
+  tex_free(t);
+  if (kind == 0) return HR_OK;
+  const int st = tex_alloc_arrays(t, kind, YL, ZL, views);
+  if (st != HR_OK) tex_free(t);
+  return st;
+}
+
+int bp_fast_tex_prepare(BpFast* f, const BpFastGeom& g) {
+  return tex_alloc(&f->tex, kFastVariants[f->variant].tex, g.YL, g.ZL, std::max(f->cap_views, g.PN));
+}
+
+// BF16 pairs of the geometry's views -> the plan's layered arrays.
+static int tex_fill(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, cudaStream_t s) {
+  const BpFastTex& t = f.tex;
+  HR_REQUIRE(t.kind == kFastVariants[f.variant].tex && t.views >= g.PN && t.YL == g.YL && t.ZL == g.ZL,
+             "fast backprojection: the textures of variant %d are not prepared", f.variant);
+  const long long rows = (long long)g.PN * g.ZL;
+  const int grid = (int)std::min<long long>(rows, 16LL * sm_count());
+  if (rows == 0) return HR_OK;
+  if (t.kind == kTexHalf) {
+    HR_CUDA_TRY(cudaMemsetAsync(t.d_scale + 1, 0, sizeof(float), s));
+    tex_absmax_kernel<<<4 * sm_count(), 256, 0, s>>>(t.d_scale, fpb, rows * g.YL);
+    tex_fill_kernel<true><<<grid, 256, 0, s>>>(t.d_scale, t.d_obj + t.n, fpb, rows, g.ZL, g.YL, t.lsh);
+  } else {
+    tex_fill_kernel<false><<<grid, 256, 0, s>>>(t.d_scale, t.d_obj + t.n, fpb, rows, g.ZL, g.YL, t.lsh);
+  }
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
 void bp_fast_destroy(BpFast* f) {
+  tex_free(&f->tex);
   for (int i = 0; i < kFastTableSets; ++i) {
     cudaFree(f->t[i].d_tab);
     cudaFree(f->t[i].d_mask);
@@ -569,6 +782,14 @@ static void launch_variant(const BpFastTables& t, const BpFast& f, const FastPar
   bp_fast_kernel<NZ, CH><<<grid, dim3(kBx, kBy), 0, s>>>(vol, fpb, ztabs(t, f), P, b_first);
 }
 
+template <int NZ>
+static void launch_tex(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol, int b_first,
+                       int b_count, cudaStream_t s) {
+  dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
+  bp_tex_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, f.tex.d_obj, f.tex.lsh, f.tex.d_scale, ztabs(t, f), P,
+                                                    b_first);
+}
+
 // Launches variant v over z blocks [b_first, b_first + b_count) (count < 0: all).
 static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, const uint32_t* fpb, int b_first,
                        int b_count, cudaStream_t s) {
@@ -578,6 +799,17 @@ static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, 
   HR_REQUIRE((g.YN + kBy - 1) / kBy <= 65535 && b_count <= 65535, "fast backprojection: grid too large");
   if (b_count == 0) return HR_OK;
   const FastParams P = make_params(g);
+  if (fv.tex) {
+    HR_REQUIRE(f.tex.kind == fv.tex && f.tex.views >= g.PN, "fast backprojection: the textures of variant %d are "
+               "not prepared", v);
+    switch (kFastNz[fv.table]) {
+      case 16: launch_tex<16>(t, f, P, vol, b_first, b_count, s); break;
+      case 8: launch_tex<8>(t, f, P, vol, b_first, b_count, s); break;
+      default: launch_tex<4>(t, f, P, vol, b_first, b_count, s); break;
+    }
+    HR_CUDA_TRY(cudaGetLastError());
+    return HR_OK;
+  }
   switch (v) {
     case 0: launch_variant<16, 0>(t, f, P, vol, fpb, b_first, b_count, s); break;
     case 1: launch_variant<16, 4>(t, f, P, vol, fpb, b_first, b_count, s); break;
@@ -688,6 +920,7 @@ int bp_fast_best_per_slice_nz(const BpFast& f) {
 }
 
 int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s) {
+  if (kFastVariants[f.variant].tex) HR_TRY(tex_fill(f, g, fpb, s));
   return run_variant(f, g, f.variant, vol, fpb, 0, -1, s);
 }
 
@@ -711,7 +944,7 @@ int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t*
   if (pin >= 0) {
     f->variant = pin;
     f->tuned = 2;
-    return HR_OK;
+    return bp_fast_tex_prepare(f, g);
   }
   cudaEvent_t e0, e1;
   HR_CUDA_TRY(cudaEventCreate(&e0));
@@ -721,10 +954,25 @@ int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t*
   float best = 1e30f;
   int best_v = f->variant;
   int st = HR_OK;
+  float fill_ms = 0.f;  // texture variants: filling the arrays, per slice of the volume
   for (int v = 0; v < kFastVariants_n && st == HR_OK; ++v) {
     const int nz = kFastNz[kFastVariants[v].table];
     const int b0 = z_first / nz;
     const int bc = std::min((band + nz - 1) / nz, f->t[kFastVariants[v].table].nblocks - b0);
+    if (kFastVariants[v].tex && f->tex.kind != kFastVariants[v].tex) {
+      f->variant = v;
+      st = bp_fast_tex_prepare(f, g);
+      for (int rep = 0; rep < 2 && st == HR_OK; ++rep) {
+        cudaEventRecord(e0, s);
+        st = tex_fill(*f, g, fpb, s);
+        cudaEventRecord(e1, s);
+        if (st == HR_OK && cudaEventSynchronize(e1) != cudaSuccess)
+          st = hr::fail(HR_ERR_CUDA, "fast backprojection autotune failed");
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        fill_ms = t / (float)std::max(g.ZN_valid, 1);
+      }
+    }
     float ms = 1e30f;
     for (int rep = 0; rep < 3 && st == HR_OK; ++rep) {
       cudaEventRecord(e0, s);
@@ -733,7 +981,7 @@ int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t*
       if (cudaEventSynchronize(e1) != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "fast backprojection autotune failed");
       float t = 0.f;
       cudaEventElapsedTime(&t, e0, e1);
-      if (rep > 0) ms = std::min(ms, t / (float)(bc * nz));  // per slice
+      if (rep > 0) ms = std::min(ms, t / (float)(bc * nz) + (kFastVariants[v].tex ? fill_ms : 0.f));  // per slice
     }
     f->tuned_ms[v] = ms;
     if (ms < best) {
@@ -743,17 +991,22 @@ int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t*
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (st != HR_OK) return st;
   f->variant = best_v;
+  if (st != HR_OK) {
+    f->variant = kFastDefaultVariant;
+    tex_free(&f->tex);
+    return st;
+  }
   f->tuned = 1;
-  return HR_OK;
+  return bp_fast_tex_prepare(f, g);
 }
 
 int bp_fast_describe(const BpFast& f, char* buf, int len) {
   if (!buf || len <= 0) return HR_OK;
   const FastVariant& fv = kFastVariants[f.variant];
   int n = snprintf(buf, (size_t)len, "slices_per_thread=%d gathers=%s tile=%dx%d %s", kFastNz[fv.table],
-                   fv.chunk < 0 ? "paired-f32x2" : fv.chunk == 0 ? "per-slice" : fv.chunk == 4 ? "chunk4" : "chunk8",
+                   fv.tex == kTexHalf ? "texture-fp16" : fv.tex == kTexFloat ? "texture-fp32"
+                   : fv.chunk < 0 ? "paired-f32x2" : fv.chunk == 0 ? "per-slice" : fv.chunk == 4 ? "chunk4" : "chunk8",
                    kBx, kBy, f.tuned == 2 ? "(pinned by HELIXRECON_BP_VARIANT)"
                    : f.tuned ? "(autotuned; ms/slice:" : "(default)");
   if (f.tuned == 1) {

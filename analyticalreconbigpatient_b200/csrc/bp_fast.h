@@ -25,12 +25,17 @@ constexpr int kFastNz[kFastTableSets] = {16, 8, 4};
 
 // Kernel variants the autotuner chooses from: table set and gather chunk
 // (0 = one slice at a time, 4/8 = slices whose gathers are issued together,
-// -1 = slice pairs in packed FP32x2 arithmetic).
+// -1 = slice pairs in packed FP32x2 arithmetic); tex != 0: the taps come from
+// the texture units' bilinear filtering of a layered copy of the filtered data
+// (kTexHalf: FP16 scaled by a power of two; kTexFloat: FP32).
+constexpr int kTexHalf = 1, kTexFloat = 2;
 struct FastVariant {
-  int table, chunk;
+  int table, chunk, tex;
 };
 constexpr FastVariant kFastVariants[] = {{0, 0}, {0, 4}, {0, 8}, {1, 0}, {1, 4}, {1, 8},
-                                         {0, -1}, {1, -1}, {2, 0}, {2, -1}, {2, 4}};
+                                         {0, -1}, {1, -1}, {2, 0}, {2, -1}, {2, 4},
+                                         {1, 0, kTexHalf}, {0, 0, kTexHalf}, {2, 0, kTexHalf},
+                                         {1, 0, kTexFloat}, {0, 0, kTexFloat}};
 constexpr int kFastVariants_n = sizeof(kFastVariants) / sizeof(kFastVariants[0]);
 constexpr int kFastDefaultVariant = 0;
 
@@ -56,6 +61,18 @@ struct BpFastHostSet {
 };
 struct BpFastHost;
 
+// Layered 2D textures holding the filtered data of the texture variants: n
+// CUDA arrays of 2^lsh views (layers) of [ZL][YL] samples each.
+struct BpFastTex {
+  int kind = 0;  // 0 (none), kTexHalf or kTexFloat
+  int lsh = 0, n = 0, YL = 0, ZL = 0, views = 0;
+  std::vector<cudaArray_t> arr;
+  std::vector<unsigned long long> tex, surf;  // texture and surface objects of the arrays
+  unsigned long long* d_obj = nullptr;        // device copy: n texture objects, then n surface objects
+  float* d_scale = nullptr;                   // device: {1 / FP16 scale, max |value| (bits)}
+  size_t bytes = 0;
+};
+
 struct BpFast {
   BpFastTables t[kFastTableSets];
   float2* d_trig = nullptr;  // per view: {cos, sin}
@@ -64,6 +81,7 @@ struct BpFast {
   int tuned = 0;
   float tuned_ms[kFastVariants_n] = {};  // autotuner: ms per slice of each variant
   size_t bytes = 0;
+  BpFastTex tex;
 };
 
 struct BpFastHost {
@@ -82,6 +100,10 @@ void bp_fast_destroy(BpFast* f);
 int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s);
 int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s);
 int bp_fast_describe(const BpFast& f, char* buf, int len);
+// Allocates (or frees) the layered textures the plan's variant samples
+// (no-op for the gather variants); hr_bp_select and the slab pipeline call it
+// after choosing a variant by hand.
+int bp_fast_tex_prepare(BpFast* f, const BpFastGeom& g);
 // Several scans in one persistent launch. Each scan runs the kernel body with
 // its own slices per thread (16, 8 or 4); batch variants differ in the CTAs
 // (of 256 threads) per SM their registers must allow (1: unconstrained; 5; 6) and in the

@@ -108,7 +108,7 @@ extern "C" int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* d
 
 extern "C" int hr_recon_describe(const hr_recon_plan* p, char* buf, int len) {
   HR_REQUIRE(p != nullptr, "hr_recon_describe: NULL plan");
-  char bp[256];
+  char bp[400];
   HR_TRY(hr_bp_describe(p->bp, bp, sizeof(bp)));
   if (buf && len > 0)
     snprintf(buf, (size_t)len, "filter=%s; backprojection: %s",

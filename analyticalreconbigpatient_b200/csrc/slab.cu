@@ -208,6 +208,7 @@ static int prepare(hr_slab_plan* p, const float* fan, bool fan_on_host) {
   HR_TRY(hr::bp_fast_autotune(&p->fast[k & 1], p->gslab, p->d_vslab, p->d_pairs, p->sc));
   p->fast[(k & 1) ^ 1].variant = p->fast[k & 1].variant;
   p->fast[(k & 1) ^ 1].tuned = p->fast[k & 1].tuned;
+  HR_TRY(hr::bp_fast_tex_prepare(&p->fast[(k & 1) ^ 1], p->gslab));
   HR_CUDA_TRY(cudaStreamSynchronize(p->sc));
   for (int b = 0; b < 2; ++b) {
     cudaGraph_t gr = nullptr;

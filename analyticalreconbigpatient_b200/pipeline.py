@@ -256,8 +256,8 @@ class StagePlans:
     def autotune(self, vol: torch.Tensor, fp: torch.Tensor, stream: int = 0) -> str:
         lib = _lib.load()
         _lib.check(lib.hr_bp_autotune(self._bp, vol.data_ptr(), fp.data_ptr(), stream))
-        buf = ctypes.create_string_buffer(256)
-        _lib.check(lib.hr_bp_describe(self._bp, buf, 256))
+        buf = ctypes.create_string_buffer(512)
+        _lib.check(lib.hr_bp_describe(self._bp, buf, 512))
         return buf.value.decode()
 
     def pack(self, out: torch.Tensor, filtered: torch.Tensor, stream: int = 0) -> None:

@@ -193,7 +193,11 @@ int hr_bp_describe(const hr_bp_plan* plan, char* buf, int len);
 /* Selects a fast-form kernel variant by index (the autotuner's candidates:
  * 0-2 sixteen slices per thread, 3-5 eight, gathers issued one, four or eight
  * slices at a time; 6-7 sixteen / eight slices per thread in packed FP32x2
- * slice pairs; 8-10 four slices per thread, per slice / pairs / batched).
+ * slice pairs; 8-10 four slices per thread, per slice / pairs / batched;
+ * 11-13 eight / sixteen / four slices per thread sampling an FP16 layered
+ * texture copy of the data with the texture units' bilinear filtering, 14-15
+ * eight / sixteen with an FP32 copy; the texture variants allocate the copy,
+ * 2 or 4 bytes per sample, and fill it on every execution).
  * For tests and manual tuning. */
 int hr_bp_select(hr_bp_plan* plan, int variant);
 

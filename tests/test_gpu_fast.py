@@ -124,7 +124,7 @@ def test_every_fast_variant_gives_the_same_volume(cuda, pixel):
     fast.pack(pairs, filt)
     lib = _lib.load()
     vols = []
-    nvar = 11
+    nvar = 16
     for v in range(nvar):
         _lib.check(lib.hr_bp_select(fast._bp, v))
         vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
@@ -138,4 +138,40 @@ def test_every_fast_variant_gives_the_same_volume(cuda, pixel):
         assert np.array_equal(vols[v], vols[0]), v
     for v in (6, 7, 9):  # packed FP32x2 rounds like FP32, but FMA contraction may differ
         assert rel_l2(vols[v], vols[0]) < 1e-6, v
+    # texture variants: the hardware blends with 1.8 fixed-point weights, an
+    # error of up to 1/256 of the neighbour difference per tap (largest, about
+    # 0.5 % of the volume, on white-noise data like these)
+    for v in (11, 12, 13, 14, 15):
+        assert rel_l2(vols[v], vols[0]) < 1e-2, (v, rel_l2(vols[v], vols[0]))
+    assert np.array_equal(vols[11], vols[12]) and np.array_equal(vols[11], vols[13])
+    assert np.array_equal(vols[14], vols[15])
     assert np.isfinite(vols[0]).all()
+
+
+@pytest.mark.parametrize("gain", [2.0**18, 2.0**-100])
+def test_fp16_texture_scales_any_data_range(cuda, gain):
+    """The FP16 texture copy is scaled by a power of two chosen from the data's
+    largest magnitude: data far outside FP16's range (overflow at 65504,
+    underflow below 6e-8) give the volume of the unit-range data times the gain
+    (a power of two, so the BF16 samples scale exactly)."""
+    from analyticalreconbigpatient_b200.pipeline import StagePlans
+
+    sc = G.Scan(ZL=16, pitch=0.9375, rotations=3, XN=24, YN=24, ZN=21, dx=2.0, dy=2.0, dz=1.0)
+    rng = np.random.default_rng(5)
+    filt = torch.tensor(rng.standard_normal((sc.PN, sc.ZL, sc.YL)).astype(np.float32), device=cuda)
+    fast = StagePlans(sc, _lib.HR_FORM_FAST)
+    lib = _lib.load()
+    out = {}
+    for name, g in (("unit", 1.0), ("scaled", gain)):
+        pairs = torch.empty((sc.PN, sc.ZL, sc.YL), dtype=torch.int32, device=cuda)
+        fast.pack(pairs, filt * g)
+        for v in (11, 14):
+            _lib.check(lib.hr_bp_select(fast._bp, v))
+            vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
+            fast.backproject(vol, pairs)
+            torch.cuda.synchronize()
+            out[name, v] = vol.cpu().numpy().astype(np.float64)
+    fast.close()
+    assert rel_l2(out["unit", 11], out["unit", 14]) < 1e-3
+    assert rel_l2(out["scaled", 11] / gain, out["unit", 11]) < 1e-6
+    assert rel_l2(out["scaled", 14] / gain, out["unit", 14]) < 1e-6
