@@ -18,7 +18,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libhelixrecon.so")
 BUILD_DIR = os.path.join(PKG, "_build")
 
-SOURCES = ["status.cpp", "capi.cpp", "recon.cpp", "rebin.cu", "filter.cu", "bp.cu", "bp_fast.cu", "filter_tc.cu", "slab.cu", "batch.cpp", "cnn.cu", "segment.cpp", "util.cu", "phantom.cu"]
+SOURCES = ["status.cpp", "capi.cpp", "recon.cpp", "rebin.cu", "filter.cu", "bp.cu", "bp_fast.cu", "filter_tc.cu", "slab.cu", "batch.cpp", "cnn.cu", "segment.cpp", "util.cu", "phantom.cu", "probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3,-fno-fast-math", "--expt-relaxed-constexpr",
               "-I" + INCLUDE, "-I" + CSRC]

@@ -24,7 +24,11 @@ struct hr_batch_plan {
   std::vector<hr_filter_tc_plan*> ftc;
   std::vector<hr_bp_plan*> bp;
   std::vector<uint32_t*> pairs;  // per scan: [PN][ZL][YL] BF16 channel pairs
-  std::vector<int> nz;           // per scan: slices per thread of its backprojection
+  std::vector<int> nz;           // per scan: slices per thread of its backprojection (register gathers)
+  std::vector<int> tv;           // per scan: its FP16 texture variant (batch variants with texture taps)
+  std::vector<int> sv;           // per scan: the variant its own autotuner chose (per-scan launches)
+  std::vector<cudaStream_t> ss;  // per scan: its stream for the per-scan launches
+  std::vector<cudaEvent_t> ready, done;  // per scan: fork and join points of the per-scan launches
   float* d_rebinned = nullptr;   // shared: the largest scan's [ViewN][YL][ZL]
   int* d_counter = nullptr;      // work-item counter of the persistent launch
   void* d_split[3] = {};         // shared tensor-core filter operands
@@ -50,6 +54,9 @@ void destroy(hr_batch_plan* p) {
   cudaFree(p->d_rebinned);
   cudaFree(p->d_counter);
   for (void* q : p->d_split) cudaFree(q);
+  for (cudaStream_t q : p->ss) cudaStreamDestroy(q);
+  for (cudaEvent_t e : p->ready) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->done) cudaEventDestroy(e);
   if (p->sc) cudaStreamDestroy(p->sc);
   delete p;
 }
@@ -60,27 +67,88 @@ int alloc(hr_batch_plan* p, void** ptr, size_t bytes) {
   return HR_OK;
 }
 
-int scans_of(const hr_batch_plan* p, float* const* vols, std::vector<hr::BpFastBatchScan>* out) {
+bool textured(int bv) { return hr::kBatchVariants[bv].tex != 0; }
+bool per_scan(int bv) { return hr::kBatchVariants[bv].streams != 0; }
+
+// The scans as batch variant bv sees them (slices per thread of its taps).
+int scans_of(const hr_batch_plan* p, float* const* vols, int bv, std::vector<hr::BpFastBatchScan>* out) {
   out->resize(p->n);
   for (int i = 0; i < p->n; ++i) {
     hr::BpFastBatchScan& b = (*out)[i];
     HR_TRY(hr::bp_plan_fast_parts(p->bp[i], &b.g, &b.f));
     b.vol = vols[i];
     b.fpb = p->pairs[i];
-    b.nz = p->nz[i];
+    const int forced = hr::kBatchVariants[bv].chunk;
+    b.nz = !textured(bv) ? p->nz[i] : forced ? forced : hr::bp_fast_variant_nz(p->tv[i]);
   }
   return HR_OK;
 }
 
+// Gives every scan's plan the variant batch variant bv runs: its own
+// autotuner's choice (per-scan launches), its FP16 texture variant (which keeps
+// a layered copy of the scan's filtered data), or a register-gather one.
+int set_scan_variants(hr_batch_plan* p, int bv) {
+  const int gather_v[3] = {0, 3, 8};  // per-slice variants with 16, 8, 4 slices per thread
+  for (int i = 0; i < p->n; ++i) {
+    int v = per_scan(bv) ? p->sv[i] : textured(bv) ? p->tv[i] : 3;
+    for (int g : gather_v)
+      if (!per_scan(bv) && !textured(bv) && hr::bp_fast_variant_nz(g) == p->nz[i]) v = g;
+    HR_TRY(hr_bp_select(p->bp[i], v));
+  }
+  return HR_OK;
+}
+
+// Per-scan launches: scan i's backprojection waits for ready[i] on the batch's
+// stream, runs on its own stream and is joined back through done[i].
+int fork_bp(const hr_batch_plan* p, int i, float* vol, cudaStream_t s) {
+  HR_CUDA_TRY(cudaEventRecord(p->ready[i], s));
+  HR_CUDA_TRY(cudaStreamWaitEvent(p->ss[i], p->ready[i], 0));
+  HR_TRY(hr_bp_execute(p->bp[i], vol, p->pairs[i], p->ss[i]));
+  HR_CUDA_TRY(cudaEventRecord(p->done[i], p->ss[i]));
+  return HR_OK;
+}
+
+int join_all(const hr_batch_plan* p, cudaStream_t s) {
+  for (int i = 0; i < p->n; ++i) HR_CUDA_TRY(cudaStreamWaitEvent(s, p->done[i], 0));
+  return HR_OK;
+}
+
+// The backprojection of batch variant bv from the scans' filtered data.
+int backproject(const hr_batch_plan* p, float* const* vols, int bv, cudaStream_t s);
+
+int fill_textures(const hr_batch_plan* p, cudaStream_t s) {
+  for (int i = 0; i < p->n; ++i) {
+    const hr::BpFastGeom* g;
+    const hr::BpFast* f;
+    HR_TRY(hr::bp_plan_fast_parts(p->bp[i], &g, &f));
+    HR_TRY(hr::bp_fast_tex_fill(*f, *g, p->pairs[i], s));
+  }
+  return HR_OK;
+}
+
+int backproject(const hr_batch_plan* p, float* const* vols, int bv, cudaStream_t s) {
+  if (per_scan(bv)) {
+    for (int i = 0; i < p->n; ++i) HR_TRY(fork_bp(p, i, vols[i], s));
+    return join_all(p, s);
+  }
+  if (textured(bv)) HR_TRY(fill_textures(p, s));
+  std::vector<hr::BpFastBatchScan> sc;
+  HR_TRY(scans_of(p, vols, bv, &sc));
+  const long long items = hr::bp_fast_batch_items(sc.data(), p->n);
+  return hr::bp_fast_batch_execute(sc.data(), p->n, bv, 0, (int)items, p->ctas[bv], p->d_counter, s);
+}
+
+// Per-scan launches start each scan's backprojection as soon as its filter
+// is done, under the next scans' rebinning and filtering (they read only the
+// scan's own filtered data).
 int enqueue(const hr_batch_plan* p, float* const* vols, const float* const* fans, cudaStream_t s) {
   for (int i = 0; i < p->n; ++i) {
     HR_TRY(hr_rebin_execute(p->rebin[i], p->d_rebinned, fans[i], s));
     HR_TRY(hr_filter_tc_execute(p->ftc[i], p->pairs[i], p->d_rebinned, HR_LAYOUT_REBIN, p->d[i].view0, s));
+    if (per_scan(p->variant)) HR_TRY(fork_bp(p, i, vols[i], s));
   }
-  std::vector<hr::BpFastBatchScan> sc;
-  HR_TRY(scans_of(p, vols, &sc));
-  const long long items = hr::bp_fast_batch_items(sc.data(), p->n);
-  return hr::bp_fast_batch_execute(sc.data(), p->n, p->variant, 0, (int)items, p->ctas[p->variant], p->d_counter, s);
+  if (per_scan(p->variant)) return join_all(p, s);
+  return backproject(p, vols, p->variant, s);
 }
 
 // Picks each scan's slices per thread with its own plan's autotuner (the
@@ -104,13 +172,20 @@ int autotune(hr_batch_plan* p) {
                                 sizeof(uint32_t) * (size_t)p->d[i].bp.PN * p->d[i].ZL * p->d[i].YL, p->sc));
   }
   p->nz.assign(p->n, 8);
+  p->tv.assign(p->n, 11);
+  p->sv.assign(p->n, 3);
   for (int i = 0; i < p->n; ++i) {
     HR_TRY(hr_bp_autotune(p->bp[i], vols[i], p->pairs[i], p->sc));
     const hr::BpFastGeom* g;
     const hr::BpFast* f;
     HR_TRY(hr::bp_plan_fast_parts(p->bp[i], &g, &f));
     p->nz[i] = hr::bp_fast_best_per_slice_nz(*f);
+    p->tv[i] = hr::bp_fast_best_tex_variant(*f);
+    p->sv[i] = f->variant;
   }
+  const int first_tex = 6;  // the texture variants follow the gather ones
+  HR_TRY(set_scan_variants(p, first_tex));
+  HR_TRY(fill_textures(p, p->sc));
   const char* pin = std::getenv("HELIXRECON_BATCH_VARIANT");
   if (pin && *pin) {
     char* end = nullptr;
@@ -119,21 +194,19 @@ int autotune(hr_batch_plan* p) {
                "HELIXRECON_BATCH_VARIANT must be an integer in [0, %d)", hr::kBatchVariants_n);
     p->variant = (int)v;
     p->tuned = 2;
-    return HR_OK;
+    return set_scan_variants(p, p->variant);
   }
-  std::vector<hr::BpFastBatchScan> sc;
-  HR_TRY(scans_of(p, vols.data(), &sc));
-  const long long items = hr::bp_fast_batch_items(sc.data(), p->n);
   cudaEvent_t e0, e1;
   HR_CUDA_TRY(cudaEventCreate(&e0));
   HR_CUDA_TRY(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_v = 0, st = HR_OK;
   for (int v = 0; v < hr::kBatchVariants_n && st == HR_OK; ++v) {
+    if (per_scan(v)) st = set_scan_variants(p, v);  // each scan's own choice (fills inside its launch)
     float ms = 1e30f;
     for (int rep = 0; rep < 2 && st == HR_OK; ++rep) {
       cudaEventRecord(e0, p->sc);
-      st = hr::bp_fast_batch_execute(sc.data(), p->n, v, 0, (int)items, p->ctas[v], p->d_counter, p->sc);
+      st = backproject(p, vols.data(), v, p->sc);  // texture fills included
       cudaEventRecord(e1, p->sc);
       if (cudaEventSynchronize(e1) != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "batch autotune: launch failed");
       float t = 0.f;
@@ -151,7 +224,7 @@ int autotune(hr_batch_plan* p) {
   if (st != HR_OK) return st;
   p->variant = best_v;
   p->tuned = 1;
-  return HR_OK;
+  return set_scan_variants(p, p->variant);
 }
 
 }  // namespace
@@ -202,7 +275,15 @@ extern "C" int hr_batch_plan_create(hr_batch_plan** plan, const hr_recon_desc* d
   }
   for (int v = 0; v < hr::kBatchVariants_n && st == HR_OK; ++v) st = hr::bp_fast_batch_grid(v, &p->ctas[v]);
   if (st == HR_OK) {
-    const cudaError_t e = cudaStreamCreateWithFlags(&p->sc, cudaStreamNonBlocking);
+    cudaError_t e = cudaStreamCreateWithFlags(&p->sc, cudaStreamNonBlocking);
+    p->ss.assign(n, nullptr);
+    p->ready.assign(n, nullptr);
+    p->done.assign(n, nullptr);
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+      e = cudaStreamCreateWithFlags(&p->ss[i], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ready[i], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->done[i], cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "hr_batch_plan_create: %s", cudaGetErrorString(e));
   }
   if (st == HR_OK) st = autotune(p);
@@ -255,17 +336,14 @@ extern "C" int hr_batch_execute(hr_batch_plan* p, float* const* d_vols, const fl
 extern "C" int hr_batch_backproject(hr_batch_plan* p, float* const* d_vols, void* stream) {
   HR_REQUIRE(p != nullptr && d_vols != nullptr, "hr_batch_backproject: NULL argument");
   for (int i = 0; i < p->n; ++i) HR_REQUIRE(d_vols[i] != nullptr, "hr_batch_backproject: NULL volume %d", i);
-  std::vector<hr::BpFastBatchScan> sc;
-  HR_TRY(scans_of(p, d_vols, &sc));
-  const long long items = hr::bp_fast_batch_items(sc.data(), p->n);
-  return hr::bp_fast_batch_execute(sc.data(), p->n, p->variant, 0, (int)items, p->ctas[p->variant], p->d_counter,
-                                   hr::as_stream(stream));
+  return backproject(p, d_vols, p->variant, hr::as_stream(stream));
 }
 
 extern "C" int hr_batch_select(hr_batch_plan* p, int variant) {
   HR_REQUIRE(p != nullptr, "hr_batch_select: NULL plan");
   HR_REQUIRE(variant >= 0 && variant < hr::kBatchVariants_n, "hr_batch_select: variant %d out of range [0, %d)",
              variant, hr::kBatchVariants_n);
+  HR_TRY(set_scan_variants(p, variant));
   p->variant = variant;
   return HR_OK;
 }
@@ -275,13 +353,22 @@ extern "C" int hr_batch_describe(const hr_batch_plan* p, char* buf, int len) {
   if (!buf || len <= 0) return HR_OK;
   std::vector<float*> vols(p->n, nullptr);
   std::vector<hr::BpFastBatchScan> sc;
-  HR_TRY(scans_of(p, vols.data(), &sc));
-  int k = snprintf(buf, (size_t)len,
-                   "%d scans, %lld work items in one persistent launch of %d CTAs (>= %d per SM, gathers %s); "
-                   "slices per thread by scan:", p->n, hr::bp_fast_batch_items(sc.data(), p->n),
-                   p->ctas[p->variant], hr::kBatchVariants[p->variant].min_ctas,
-                   hr::kBatchVariants[p->variant].chunk > 0 ? "in chunks of 4 slices" : "per slice");
-  for (int i = 0; i < p->n && k > 0 && k < len; ++i) k += snprintf(buf + k, (size_t)(len - k), " %d", p->nz[i]);
+  HR_TRY(scans_of(p, vols.data(), p->variant, &sc));
+  const hr::BatchVariant& bv = hr::kBatchVariants[p->variant];
+  int k = 0;
+  if (bv.streams) {
+    k = snprintf(buf, (size_t)len, "%d scans, each scan's own backprojection on a stream of its own (fork/join in "
+                 "the graph); variant by scan:", p->n);
+    for (int i = 0; i < p->n && k > 0 && k < len; ++i) k += snprintf(buf + k, (size_t)(len - k), " %d", p->sv[i]);
+  } else {
+    k = snprintf(buf, (size_t)len,
+                 "%d scans, %lld work items in one persistent launch of %d CTAs (>= %d per SM, taps %s); "
+                 "slices per thread by scan:", p->n, hr::bp_fast_batch_items(sc.data(), p->n),
+                 p->ctas[p->variant], bv.min_ctas,
+                 bv.tex ? "from FP16 textures" : bv.chunk > 0 ? "gathered in chunks of 4 slices"
+                 : "gathered per slice");
+    for (int i = 0; i < p->n && k > 0 && k < len; ++i) k += snprintf(buf + k, (size_t)(len - k), " %d", sc[i].nz);
+  }
   if (k > 0 && k < len)
     k += snprintf(buf + k, (size_t)(len - k), " %s",
                   p->tuned == 2 ? "(pinned by HELIXRECON_BATCH_VARIANT)"
@@ -304,6 +391,11 @@ extern "C" size_t hr_batch_device_bytes(const hr_batch_plan* p) {
   if (!p) return 0;
   size_t b = p->bytes;
   for (auto* f : p->ftc) b += hr_filter_tc_device_bytes(f);
+  for (auto* q : p->bp) {
+    const hr::BpFastGeom* g;
+    const hr::BpFast* f;
+    if (hr::bp_plan_fast_parts(q, &g, &f) == HR_OK) b += hr::bp_fast_device_bytes(*f);
+  }
   return b;
 }
 

@@ -338,9 +338,17 @@ __global__ void __launch_bounds__(kBx* kBy) bp_fast_kernel(float* __restrict__ v
 // scheduler; a static round robin lets CTAs drift apart and spreads the
 // window over many z blocks. Each scan keeps the slices per thread its own
 // geometry favours (16, 8 or 4: a uniform branch per item).
+// Per-scan texture handles of the texture variants.
+struct TexRef {
+  const unsigned long long* texs;  // texture object of each array of 2^lsh views
+  const float* scale;              // {1 / FP16 scale, ...}
+  int lsh;
+};
+
 struct BatchScan {
   FastParams P;
   ZTabs T;
+  TexRef X;
   float* vol;
   const uint32_t* fpb;
   int tiles_x, tiles_y, item0, nz;
@@ -438,15 +446,11 @@ __global__ void tex_fill_kernel(float* __restrict__ scale, const unsigned long l
 // Same tables, window masks and weight as fast_column; the tap is a texture
 // sample. The NZ samples of a (column, view) are issued before any is used.
 template <int NZ>
-__global__ void __launch_bounds__(kBx* kBy) bp_tex_kernel(float* __restrict__ vol,
-                                                         const unsigned long long* __restrict__ texs, int lsh,
-                                                         const float* __restrict__ scale, const ZTabs T,
-                                                         const FastParams P, int b_first) {
+__device__ __forceinline__ void tex_column(float* __restrict__ vol, const TexRef& X, const ZTabs& T,
+                                           const FastParams& P, int xi, int yi, int b) {
   static_assert(NZ % 2 == 0, "table entries are read two slices at a time");
-  const int xi = blockIdx.x * kBx + threadIdx.x;
-  const int yi = blockIdx.y * kBy + threadIdx.y;
-  if (xi >= P.XN || yi >= P.YN) return;
-  const int b = b_first + blockIdx.z;
+  const unsigned long long* __restrict__ texs = X.texs;
+  const int lsh = X.lsh;
   const int z0 = b * NZ;
   const int2 blk = T.zblock[b];
   const int off = T.zoff[b];
@@ -495,11 +499,53 @@ __global__ void __launch_bounds__(kBx* kBy) bp_tex_kernel(float* __restrict__ vo
 #pragma unroll
     for (int m = 0; m < NZ; ++m) res[m] = fmaf(rcp_approx(fmaf(qv[m], E, 1.0f)), tap[m], res[m]);
   }
-  const float outs = P.DeltaFai * __ldg(scale);
+  const float outs = P.DeltaFai * __ldg(X.scale);
   float* out = vol + ((size_t)yi * P.XN + xi) * P.ZN + z0;
 #pragma unroll
   for (int m = 0; m < NZ; ++m)
     if (z0 + m < P.ZN) out[m] = res[m] * outs;
+}
+
+template <int NZ>
+__global__ void __launch_bounds__(kBx* kBy) bp_tex_kernel(float* __restrict__ vol, const TexRef X, const ZTabs T,
+                                                         const FastParams P, int b_first) {
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  if (xi >= P.XN || yi >= P.YN) return;
+  tex_column<NZ>(vol, X, T, P, xi, yi, b_first + blockIdx.z);
+}
+
+// The persistent multi-scan launch with texture taps: the work items and
+// their claiming as in bp_fast_batch_kernel; each scan samples its own arrays
+// with 8 or 4 slices per thread (NZF = 0: the scan's own choice) or 4 for all
+// scans (NZF = 4: the smaller body leaves registers for the scan parameters,
+// which a dynamic scan index keeps out of the constant-operand path).
+template <int MB, int NZF>
+__global__ void __launch_bounds__(kBx* kBy, MB) bp_tex_batch_kernel(const __grid_constant__ BatchParams B) {
+  __shared__ int s_item;
+  const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
+  for (;;) {
+    if (leader) s_item = atomicAdd(B.counter, 1);
+    __syncthreads();
+    const int k = s_item;
+    __syncthreads();
+    if (k >= B.count) break;
+    const int item = B.begin + k;
+    int sc = 0;
+    while (sc + 1 < B.n && item >= B.s[sc + 1].item0) ++sc;
+    const BatchScan& S = B.s[sc];
+    const int local = item - S.item0;
+    const int t = local / S.tiles_x;
+    const int xi = (local - t * S.tiles_x) * kBx + threadIdx.x;
+    const int yi = (t % S.tiles_y) * kBy + threadIdx.y;
+    const int b = t / S.tiles_y;
+    if (xi < S.P.XN && yi < S.P.YN) {
+      if (NZF == 0 && S.nz == 8)
+        tex_column<8>(S.vol, S.X, S.T, S.P, xi, yi, b);
+      else
+        tex_column<4>(S.vol, S.X, S.T, S.P, xi, yi, b);
+    }
+  }
 }
 
 // fp32 [n][YL] rows -> BF16 pairs (u, u+1), round to nearest even.
@@ -728,9 +774,9 @@ int bp_fast_tex_prepare(BpFast* f, const BpFastGeom& g) {
 }
 
 // BF16 pairs of the geometry's views -> the plan's layered arrays.
-static int tex_fill(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, cudaStream_t s) {
+int bp_fast_tex_fill(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, cudaStream_t s) {
   const BpFastTex& t = f.tex;
-  HR_REQUIRE(t.kind == kFastVariants[f.variant].tex && t.views >= g.PN && t.YL == g.YL && t.ZL == g.ZL,
+  HR_REQUIRE(t.kind != 0 && t.views >= g.PN && t.YL == g.YL && t.ZL == g.ZL,
              "fast backprojection: the textures of variant %d are not prepared", f.variant);
   const long long rows = (long long)g.PN * g.ZL;
   const int grid = (int)std::min<long long>(rows, 16LL * sm_count());
@@ -771,6 +817,8 @@ static FastParams make_params(const BpFastGeom& g) {
   return P;
 }
 
+static TexRef texref(const BpFast& f) { return TexRef{f.tex.d_obj, f.tex.d_scale, f.tex.lsh}; }
+
 static ZTabs ztabs(const BpFastTables& t, const BpFast& f) {
   return ZTabs{f.d_trig, t.d_tab, t.d_mask, reinterpret_cast<const int2*>(t.d_zblock), t.d_zblock + 2 * t.nblocks};
 }
@@ -786,8 +834,7 @@ template <int NZ>
 static void launch_tex(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol, int b_first,
                        int b_count, cudaStream_t s) {
   dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
-  bp_tex_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, f.tex.d_obj, f.tex.lsh, f.tex.d_scale, ztabs(t, f), P,
-                                                    b_first);
+  bp_tex_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), P, b_first);
 }
 
 // Launches variant v over z blocks [b_first, b_first + b_count) (count < 0: all).
@@ -858,6 +905,19 @@ static int batch_launch(const BatchParams* B, int* ctas, cudaStream_t s) {
   return HR_OK;
 }
 
+template <int MB, int NZF>
+static int batch_launch_tex(const BatchParams* B, int* ctas, cudaStream_t s) {
+  if (ctas) {
+    int per_sm = 0;
+    HR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_tex_batch_kernel<MB, NZF>, kBx * kBy, 0));
+    *ctas = std::max(per_sm, 1) * sm_count();
+    return HR_OK;
+  }
+  bp_tex_batch_kernel<MB, NZF><<<B->grid, dim3(kBx, kBy), 0, s>>>(*B);
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
 // ctas != nullptr: report the resident CTAs of batch variant bv; else launch *B.
 static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t s) {
   switch (bv) {
@@ -867,6 +927,17 @@ static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t 
     case 3: return batch_launch<1, 4>(B, ctas, s);
     case 4: return batch_launch<5, 4>(B, ctas, s);
     case 5: return batch_launch<6, 4>(B, ctas, s);
+    case 6: return batch_launch_tex<1, 0>(B, ctas, s);
+    case 7: return batch_launch_tex<4, 0>(B, ctas, s);
+    case 8: return batch_launch_tex<4, 4>(B, ctas, s);
+    case 9: return batch_launch_tex<5, 4>(B, ctas, s);
+    case 10: return batch_launch_tex<6, 4>(B, ctas, s);
+    case 11:  // per-scan launches: no persistent grid
+      if (ctas) {
+        *ctas = 0;
+        return HR_OK;
+      }
+      return hr::fail(HR_ERR_INVALID_ARGUMENT, "batch backprojection: variant 11 is not a persistent launch");
     default: return hr::fail(HR_ERR_INVALID_ARGUMENT, "batch backprojection: unknown variant %d", bv);
   }
 }
@@ -891,6 +962,12 @@ int bp_fast_batch_execute(const BpFastBatchScan* scans, int n, int bv, int begin
     S.T = ztabs(t, *scans[i].f);
     S.vol = scans[i].vol;
     S.fpb = scans[i].fpb;
+    S.X = texref(*scans[i].f);
+    HR_REQUIRE(!kBatchVariants[bv].tex || (scans[i].f->tex.kind == kTexHalf && scans[i].f->tex.views >= g.PN &&
+                                           (scans[i].nz == 8 || scans[i].nz == 4)),
+               "batch backprojection: scan %d has no FP16 texture copy for variant %d", i, bv);
+    HR_REQUIRE(!kBatchVariants[bv].tex || kBatchVariants[bv].chunk == 0 || scans[i].nz == kBatchVariants[bv].chunk,
+               "batch backprojection: variant %d runs %d slices per thread", bv, kBatchVariants[bv].chunk);
     S.tiles_x = (g.XN + kBx - 1) / kBx;
     S.tiles_y = (g.YN + kBy - 1) / kBy;
     S.item0 = (int)item0;
@@ -910,6 +987,13 @@ int bp_fast_batch_execute(const BpFastBatchScan* scans, int n, int bv, int begin
   return batch_dispatch(bv, &B, nullptr, s);
 }
 
+int bp_fast_best_tex_variant(const BpFast& f) {
+  // FP16 texture variants with 8 (11) and 4 (13) slices per thread
+  return f.tuned == 1 && f.tuned_ms[13] < f.tuned_ms[11] ? 13 : 11;
+}
+
+int bp_fast_variant_nz(int v) { return v >= 0 && v < kFastVariants_n ? kFastNz[kFastVariants[v].table] : 0; }
+
 int bp_fast_best_per_slice_nz(const BpFast& f) {
   // per-slice variants of each table set: 0 (16), 3 (8), 8 (4)
   const int cand[3] = {0, 3, 8};
@@ -920,7 +1004,7 @@ int bp_fast_best_per_slice_nz(const BpFast& f) {
 }
 
 int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s) {
-  if (kFastVariants[f.variant].tex) HR_TRY(tex_fill(f, g, fpb, s));
+  if (kFastVariants[f.variant].tex) HR_TRY(bp_fast_tex_fill(f, g, fpb, s));
   return run_variant(f, g, f.variant, vol, fpb, 0, -1, s);
 }
 
@@ -964,7 +1048,7 @@ int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t*
       st = bp_fast_tex_prepare(f, g);
       for (int rep = 0; rep < 2 && st == HR_OK; ++rep) {
         cudaEventRecord(e0, s);
-        st = tex_fill(*f, g, fpb, s);
+        st = bp_fast_tex_fill(*f, g, fpb, s);
         cudaEventRecord(e1, s);
         if (st == HR_OK && cudaEventSynchronize(e1) != cudaSuccess)
           st = hr::fail(HR_ERR_CUDA, "fast backprojection autotune failed");

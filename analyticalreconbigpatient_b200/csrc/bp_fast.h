@@ -89,6 +89,9 @@ struct BpFastHost {
   std::vector<float2> trig;
 };
 
+// Device bytes the plan holds: tables and, for a texture variant, the layered copy.
+inline size_t bp_fast_device_bytes(const BpFast& f) { return f.bytes + f.tex.bytes; }
+
 int bp_fast_create(BpFast* f, const BpFastGeom& g, const double* w);
 // Pieces of bp_fast_create for plans whose geometry changes between launches
 // (z slabs): build the tables of a geometry on the host, reserve device
@@ -104,14 +107,24 @@ int bp_fast_describe(const BpFast& f, char* buf, int len);
 // (no-op for the gather variants); hr_bp_select and the slab pipeline call it
 // after choosing a variant by hand.
 int bp_fast_tex_prepare(BpFast* f, const BpFastGeom& g);
+// Fills the plan's layered textures from BF16 pairs (stream-ordered).
+int bp_fast_tex_fill(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, cudaStream_t s);
 // Several scans in one persistent launch. Each scan runs the kernel body with
-// its own slices per thread (16, 8 or 4); batch variants differ in the CTAs
-// (of 256 threads) per SM their registers must allow (1: unconstrained; 5; 6) and in the
-// gathers issued together (one slice at a time, or chunks of 4 slices).
+// its own slices per thread (16, 8 or 4; 8 or 4 with texture taps); batch
+// variants differ in the CTAs (of 256 threads) per SM their registers must
+// allow (1: unconstrained; 4; 5; 6), in the gathers issued together (one slice
+// at a time, or chunks of 4 slices) and in the taps (register gathers, or
+// samples of each scan's FP16 texture copy; for these, chunk = 4 runs every
+// scan with 4 slices per thread). The last variant (streams = 1) is not a
+// persistent launch: every scan runs its own plan's kernel on a stream of its
+// own, forked from and joined back into the batch's stream (the batch plan
+// drives it; bp_fast_batch_execute refuses it).
 struct BatchVariant {
-  int min_ctas, chunk;
+  int min_ctas, chunk, tex, streams;
 };
-constexpr BatchVariant kBatchVariants[] = {{1, 0}, {5, 0}, {6, 0}, {1, 4}, {5, 4}, {6, 4}};
+constexpr BatchVariant kBatchVariants[] = {{1, 0}, {5, 0}, {6, 0}, {1, 4}, {5, 4}, {6, 4},
+                                           {1, 0, kTexHalf}, {4, 0, kTexHalf}, {4, 4, kTexHalf},
+                                           {5, 4, kTexHalf}, {6, 4, kTexHalf}, {0, 0, 0, 1}};
 constexpr int kBatchVariants_n = sizeof(kBatchVariants) / sizeof(kBatchVariants[0]);
 struct BpFastBatchScan {
   const BpFast* f;
@@ -130,6 +143,10 @@ int bp_fast_batch_execute(const BpFastBatchScan* scans, int n, int bv, int begin
                           int* d_counter, cudaStream_t s);
 // Slices per thread of the fastest per-slice variant the plan's autotuner timed (8 if untuned).
 int bp_fast_best_per_slice_nz(const BpFast& f);
+// The faster of the FP16 texture variants with 8 and 4 slices per thread (11 if untuned).
+int bp_fast_best_tex_variant(const BpFast& f);
+// Slices per thread of variant v.
+int bp_fast_variant_nz(int v);
 // The fast-form geometry and tables of a backprojection plan (HR_FORM_FAST).
 int bp_plan_fast_parts(const hr_bp_plan* plan, const BpFastGeom** g, const BpFast** f);
 // FP32 rows [rows][YL] -> BF16 channel pairs: word u = bf16(x[u]) | bf16(x[u+1]) << 16.

@@ -146,7 +146,12 @@ extern "C" int hr_recon_check(const hr_recon_plan* p) {
 }
 
 extern "C" size_t hr_recon_device_bytes(const hr_recon_plan* p) {
-  return p ? p->bytes + (p->filter_tc ? hr_filter_tc_device_bytes(p->filter_tc) : 0) : 0;
+  if (!p) return 0;
+  size_t b = p->bytes + (p->filter_tc ? hr_filter_tc_device_bytes(p->filter_tc) : 0);
+  const hr::BpFastGeom* g;
+  const hr::BpFast* f;
+  if (p->d.form == HR_FORM_FAST && hr::bp_plan_fast_parts(p->bp, &g, &f) == HR_OK) b += hr::bp_fast_device_bytes(*f);
+  return b;
 }
 
 extern "C" void hr_recon_plan_destroy(hr_recon_plan* p) { destroy(p); }

@@ -269,7 +269,8 @@ extern "C" int hr_slab_describe(const hr_slab_plan* p, char* buf, int len) {
 
 extern "C" size_t hr_slab_device_bytes(const hr_slab_plan* p) {
   if (!p) return 0;
-  return p->bytes + p->fast[0].bytes + p->fast[1].bytes + hr_filter_tc_device_bytes(p->ftc);
+  return p->bytes + hr::bp_fast_device_bytes(p->fast[0]) + hr::bp_fast_device_bytes(p->fast[1]) +
+         hr_filter_tc_device_bytes(p->ftc);
 }
 
 extern "C" void hr_slab_plan_destroy(hr_slab_plan* p) { destroy(p); }

@@ -25,6 +25,7 @@ bounded sample of the same workload, on all host cores.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -549,27 +550,40 @@ def run_batch(args, dev, world, rank, barrier):
                          "dz_mm": round(sc.dz, 4), "updates": sc.updates(), "hu_rmse_vs_plain_solo": hu})
     pk, pk_kind = peaks()
     ach = BYTES_PER_UPDATE_BF16 * updates / (bp_ms * 1e-3) / 1e9
+    n = len(scans)
+    if "persistent launch" in desc:
+        textured = "FP16 textures" in desc
+        bp_kernel = "bp_tex_batch_kernel" if textured else "bp_fast_batch_kernel"
+        how = "one persistent backprojection launch"
+        bp_launches = 1 + (2 * n if textured else 0)  # + the FP16 scale and fill kernels per scan
+    else:
+        solo_v = [int(t) for t in desc.split("variant by scan:")[1].split("(")[0].split()]
+        n_tex = sum(v >= 11 for v in solo_v)
+        bp_kernel = "bp_tex_kernel" if n_tex else "bp_fast_kernel"
+        bp_kernel += " per scan, on parallel streams"
+        how = "each scan's backprojection on a stream of its own"
+        bp_launches = n + 2 * n_tex
     line = {"metric": "GUPS (voxel-view updates/s, rebin+filter+3D-weighted helical BP)",
             "value": updates * world / (ms * 1e-3) / 1e9, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "s_per_batch": ms * 1e-3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
             "data": "synthetic (analytic FP64 projections of 60 seeded random ellipsoids per scan, Poisson noise "
                     "at I0=2e5 before the log)",
-            "form": "fast (uneven batch, one persistent backprojection launch)",
+            "form": f"fast (uneven batch, {how})",
             "config": {"workload": f"{len(scans)} uneven helical scans (888-channel curved detector, 984 views/rot; "
                                    "rotations 2..30, rows 16/32/64, pitch 0.5/0.9375/1.375, 256^2 or 512^2 x 32..400 "
                                    "slices; seed 6)",
                        "updates_per_batch": updates, "fan_bytes": sum(sc.projection_bytes() for sc in scans),
                        "flush": "inputs larger than L2 (22 GB of fan data)"},
-            "roofline": {"bound": "hbm", "kernel": "bp_fast_batch_kernel", "achieved": ach, "peak": pk["hbm_gbs"],
+            "roofline": {"bound": "hbm", "kernel": bp_kernel, "achieved": ach, "peak": pk["hbm_gbs"],
                          "unit": "GB/s", "frac": ach / pk["hbm_gbs"], "peak_source": pk_kind, "traffic": None,
                          "backprojection_ms": bp_ms,
-                         "note": "gather-equivalent bytes (8 B/update) / persistent backprojection time"},
+                         "note": "gather-equivalent bytes (8 B/update) / batch backprojection time"},
             "e2e": {"value": updates * world / e2e_s / 1e9, "unit": "GUPS", "s_per_batch": e2e_s,
                     "h2d_bytes_per_step": sum(sc.projection_bytes() for sc in scans),
                     "d2h_bytes_per_step": sum(sc.volume_bytes() for sc in scans),
                     "entry": "BatchRecon.run with pinned host copies in and out"},
-            "gpu_launches": (3 * len(scans) + 1) * args.steps,
+            "gpu_launches": (3 * n + bp_launches) * args.steps,
             "solo_fast_sum_ms": solo_ms, "batch_speedup_vs_solo": solo_ms / ms,
             "max_hu_rmse_vs_plain_solo": max(p["hu_rmse_vs_plain_solo"] for p in per_scan),
             "per_scan": per_scan, "kernels": desc, "clocks": clocks.summary()}
@@ -779,7 +793,8 @@ def main():
     pk, pk_kind = peaks()
     bp_ms = res["stages_ms"]["backprojection"]
     bytes_per_update = BYTES_PER_UPDATE_BF16 if chosen == _lib.HR_FORM_FAST else BYTES_PER_UPDATE_FP32
-    kname = "bp_fast_kernel" if chosen == _lib.HR_FORM_FAST else "bp_plain_kernel"
+    textured = chosen == _lib.HR_FORM_FAST and "texture" in res["kernels"]
+    kname = ("bp_tex_kernel" if textured else "bp_fast_kernel") if chosen == _lib.HR_FORM_FAST else "bp_plain_kernel"
     achieved = bytes_per_update * updates / (bp_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": pk_kind,
@@ -789,6 +804,20 @@ def main():
                 "note": "gather-equivalent bytes (4 taps per update: 16 B FP32, 8 B BF16) / backprojection kernel "
                         "time; the backprojection is gather/issue bound, its compulsory DRAM bytes are only the "
                         "filtered data and the volume"}
+    if textured:
+        # the taps come from the texture units' bilinear filtering (one sample per update), whose
+        # rate on this device the library measures; the backprojection time includes filling the
+        # layered FP16 copy of the filtered data
+        rate = ctypes.c_double(0.0)
+        _lib.check(_lib.load().hr_texture_sample_rate(ctypes.byref(rate), 0))
+        samples = updates / (bp_ms * 1e-3) / 1e9
+        roofline["texture"] = {"achieved": samples, "peak": rate.value / 1e9, "unit": "Gsample/s",
+                               "frac": samples * 1e9 / rate.value if rate.value > 0 else None,
+                               "peak_source": "measured (hr_texture_sample_rate: cache-resident FP16 layered "
+                                              "texture, every lane active)"}
+        roofline["note"] = ("gather-equivalent bytes (4 FP16 taps = 8 B per update) / backprojection time "
+                            "(texture fill included); the taps are bilinear texture samples, so the bound is the "
+                            "texture units' sample rate (roofline.texture), not HBM")
 
     line = {"metric": "GUPS (voxel-view updates/s, rebin+filter+3D-weighted helical BP)", "value": value,
             "unit": "GUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,

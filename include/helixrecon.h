@@ -221,6 +221,13 @@ int hr_bp_plain_noalloc(float* d_vol, const float* d_fp, const float* d_w, const
  * backprojection plan reads this layout. */
 int hr_pack_bf16_pairs(uint32_t* d_out, const float* d_in, long long rows, int YL, void* stream);
 
+/* ---- device probe -------------------------------------------------------- */
+/* No counterpart in the reference. Measures the texture units' rate of
+ * bilinear samples from an FP16 layered texture (samples per second over the
+ * whole device, cache-resident texture, every lane active): the roofline of
+ * the texture-sampling backprojection variants. Synchronises the stream. */
+int hr_texture_sample_rate(double* samples_per_s, void* stream);
+
 /* ---- whole chain: rebin -> crop -> preweight/filter -> backprojection ---- */
 /* The per-scan driver of src/analyticalReconBigPatient.m:77-146 as one plan. */
 typedef struct hr_recon_desc {
@@ -289,8 +296,15 @@ int hr_batch_execute(hr_batch_plan* plan, float* const* d_vols, const float* con
 int hr_batch_backproject(hr_batch_plan* plan, float* const* d_vols, void* stream);
 /* Selects a batch backprojection variant (0..5: registers unconstrained, or
  * limited for 5 or 6 CTAs of 256 threads per SM; gathers per slice (0..2) or in
- * chunks of 4 slices (3..5)); each scan keeps the slices per thread its own
- * autotuner chose. */
+ * chunks of 4 slices (3..5); 6..10: taps sampled from each scan's FP16 layered
+ * texture copy, with each scan's own slices per thread and registers
+ * unconstrained or limited for 4 CTAs per SM (6, 7), or 4 slices per thread
+ * for every scan and registers limited for 4, 5 or 6 CTAs per SM (8..10));
+ * 11: no persistent launch, every scan's own plan kernel on a stream of its
+ * own, forked after the scan's filter (under the next scans' rebinning and
+ * filtering) and joined at the end. The gather variants keep the slices per
+ * thread each scan's own autotuner chose. Switching variants allocates or
+ * frees the scans' texture copies. */
 int hr_batch_select(hr_batch_plan* plan, int variant);
 int hr_batch_describe(const hr_batch_plan* plan, char* buf, int len);
 int hr_batch_check(const hr_batch_plan* plan);

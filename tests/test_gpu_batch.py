@@ -53,9 +53,15 @@ def solo(scan, fan, fast_variant):
 
 # slices per thread -> the solo per-slice variant with the same kernel body
 NZ_TO_FAST = {16: 0, 8: 3, 4: 8}
+# batch variants with texture taps: the solo FP16 texture variants
+NZ_TO_TEX = {8: 11, 4: 13}
+TEXTURED = (6, 7, 8, 9, 10)
 
 
-@pytest.mark.parametrize("bv", [0, 1, 2, 3, 5])
+PER_SCAN = 11  # each scan's own kernel on a stream of its own
+
+
+@pytest.mark.parametrize("bv", [0, 1, 2, 3, 5, 6, 7, 9, PER_SCAN])
 def test_batch_equals_each_scan_alone(cuda, bv):
     scans = uneven_scans()
     fans = fans_for(scans, noise=True)
@@ -66,11 +72,17 @@ def test_batch_equals_each_scan_alone(cuda, bv):
     torch.cuda.synchronize()
     rec.check()
     desc = rec.describe()
-    nzs = [int(t) for t in desc.split("slices per thread by scan:")[1].split("(")[0].split()]
-    assert len(nzs) == len(scans) and set(nzs) <= {16, 8, 4}, desc
-    for sc, fan, v, nz in zip(scans, fans, vols, nzs):
+    if bv == PER_SCAN:
+        solo_variants = [int(t) for t in desc.split("variant by scan:")[1].split("(")[0].split()]
+        assert len(solo_variants) == len(scans), desc
+    else:
+        nzs = [int(t) for t in desc.split("slices per thread by scan:")[1].split("(")[0].split()]
+        assert len(nzs) == len(scans) and set(nzs) <= ({8, 4} if bv in TEXTURED else {16, 8, 4}), desc
+        assert ("FP16 textures" in desc) == (bv in TEXTURED), desc
+        solo_variants = [(NZ_TO_TEX if bv in TEXTURED else NZ_TO_FAST)[nz] for nz in nzs]
+    for sc, fan, v, sv in zip(scans, fans, vols, solo_variants):
         got = v.cpu().numpy()
-        ref = solo(sc, fan, NZ_TO_FAST[nz])
+        ref = solo(sc, fan, sv)
         assert np.isfinite(got).all(), rec.describe()
         assert np.count_nonzero(ref) > ref.size // 2
         assert rel_l2(got, ref) < 1e-6, (sc, rec.describe())
@@ -103,7 +115,7 @@ def test_batch_graph_replay_and_new_buffers(cuda):
 def test_batch_autotuner_reports_every_variant(cuda):
     rec = BatchRecon(uneven_scans()[:2])
     desc = rec.describe()
-    assert "autotuned" in desc and all(f"v{v}=" in desc for v in range(6)), desc
+    assert "autotuned" in desc and all(f"v{v}=" in desc for v in range(12)), desc
     rec.close()
 
 

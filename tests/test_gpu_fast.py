@@ -175,3 +175,14 @@ def test_fp16_texture_scales_any_data_range(cuda, gain):
     assert rel_l2(out["unit", 11], out["unit", 14]) < 1e-3
     assert rel_l2(out["scaled", 11] / gain, out["unit", 11]) < 1e-6
     assert rel_l2(out["scaled", 14] / gain, out["unit", 14]) < 1e-6
+
+
+def test_texture_sample_rate_probe(cuda):
+    """The texture-rate probe (the roofline of the texture variants) returns a
+    device-wide bilinear sample rate of the right order for a B200: 148 SMs,
+    up to four samples per SM per clock at ~2 GHz."""
+    import ctypes
+
+    rate = ctypes.c_double(0.0)
+    _lib.check(_lib.load().hr_texture_sample_rate(ctypes.byref(rate), 0))
+    assert 1e11 < rate.value < 4e12, rate.value
