@@ -41,6 +41,7 @@ constexpr int kBx = 8, kBy = 32;  // CTA tile (x, y): 8 warps of 8 x 4 columns
 constexpr double kTwoPiTrunc = 2.0 * 3.14159265358979;
 constexpr double kInvTwoPi = 1.0 / (2.0 * 3.141592653589793);
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: adding it rounds to an integer
+constexpr float kFarT2 = 1e30f;         // table t2 of a slice that does not have the view
 
 __device__ __forceinline__ float ex2_approx(float x) {
   float y;
@@ -492,7 +493,7 @@ __device__ __forceinline__ void tex_column(float* __restrict__ vol, const TexRef
       for (int i = 0; i < 2; ++i) {
         const int m = 2 * c + i;
         const float vh = fmaf(i ? t.z : t.x, K, zlch);  // row position + 1/2
-        const bool ok = ((mask >> m) & 1u) && vh >= 0.5f && vh < vtop;  // floor in [0, ZL-2]
+        const bool ok = vh >= 0.5f && vh < vtop;  // floor in [0, ZL-2]; false for slices without the view
         tap[m] = ok ? tex2DLayered<float>(tx, xt, vh, layer) : 0.0f;
       }
     }
@@ -610,7 +611,10 @@ static int build_host(BpFastHostSet* t, int NZ, const BpFastGeom& g, const doubl
     total += (size_t)(e - a + 1);
   }
   HR_REQUIRE(total < (1ull << 31) / NZ, "fast backprojection: z-block table too large");
-  t->tab.assign(total * NZ, make_float2(0.f, 0.f));
+  // slices without the view: t2 far outside any detector (the texture variants'
+  // row test rejects them without the mask; finite, so masked-out blends of the
+  // gather variants stay finite before their zero weight)
+  t->tab.assign(total * NZ, make_float2(kFarT2, 0.f));
   t->mask.assign(total, 0u);
   for (int b = 0; b < nblocks; ++b) {
     for (int q = 0; q < t->zb[2 * b + 1]; ++q) {
