@@ -16,8 +16,10 @@
 // backprojection tables, so one captured CUDA graph -- rebin, preweight/split,
 // tensor-core filter, backprojection -- serves every slab of a buffer parity.
 // Fan windows are copied into ping-pong buffers on a second stream while the
-// previous slab computes; each slab's tables are built on the host in FP64 and
-// uploaded in stream order before its graph launch.
+// previous slab computes, and each slab's volume leaves its own ping-pong
+// buffer on a third stream while the next slab computes; each slab's tables
+// are built on the host in FP64 and uploaded in stream order before its graph
+// launch.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -38,9 +40,10 @@ struct hr_slab_plan {
   float* d_fan[2] = {nullptr, nullptr};
   float* d_reb = nullptr;
   uint32_t* d_pairs = nullptr;
-  float* d_vslab = nullptr;
-  cudaStream_t sc = nullptr, scopy = nullptr;
+  float* d_vslab[2] = {nullptr, nullptr};
+  cudaStream_t sc = nullptr, scopy = nullptr, sout = nullptr;
   cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
+  cudaEvent_t computed[2] = {nullptr, nullptr}, drained[2] = {nullptr, nullptr};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   size_t bytes = 0;
 };
@@ -59,16 +62,19 @@ void destroy(hr_slab_plan* p) {
     if (p->graph[i]) cudaGraphExecDestroy(p->graph[i]);
     hr::bp_fast_destroy(&p->fast[i]);
     cudaFree(p->d_fan[i]);
+    cudaFree(p->d_vslab[i]);
     if (p->copied[i]) cudaEventDestroy(p->copied[i]);
     if (p->consumed[i]) cudaEventDestroy(p->consumed[i]);
+    if (p->computed[i]) cudaEventDestroy(p->computed[i]);
+    if (p->drained[i]) cudaEventDestroy(p->drained[i]);
   }
   hr_rebin_plan_destroy(p->rebin);
   hr_filter_tc_plan_destroy(p->ftc);
   cudaFree(p->d_reb);
   cudaFree(p->d_pairs);
-  cudaFree(p->d_vslab);
   if (p->sc) cudaStreamDestroy(p->sc);
   if (p->scopy) cudaStreamDestroy(p->scopy);
+  if (p->sout) cudaStreamDestroy(p->sout);
   delete p;
 }
 
@@ -103,7 +109,7 @@ int enqueue_fan_copy(hr_slab_plan* p, int k, const float* fan, bool fan_on_host)
 int slab_kernels(hr_slab_plan* p, int b, cudaStream_t s) {
   HR_TRY(hr_rebin_execute(p->rebin, p->d_reb, p->d_fan[b], s));
   HR_TRY(hr_filter_tc_execute(p->ftc, p->d_pairs, p->d_reb, HR_LAYOUT_REBIN, p->margin, s));
-  return hr::bp_fast_execute(p->fast[b], p->gslab, p->d_vslab, p->d_pairs, s);
+  return hr::bp_fast_execute(p->fast[b], p->gslab, p->d_vslab[b], p->d_pairs, s);
 }
 
 }  // namespace
@@ -176,13 +182,16 @@ extern "C" int hr_slab_plan_create(hr_slab_plan** plan, const hr_recon_desc* d, 
   for (int b = 0; b < 2 && st == HR_OK; ++b) st = alloc(p, (void**)&p->d_fan[b], (size_t)p->Wfan * per_view * 4);
   if (st == HR_OK) st = alloc(p, (void**)&p->d_reb, (size_t)p->Wfan * per_view * 4);
   if (st == HR_OK) st = alloc(p, (void**)&p->d_pairs, (size_t)p->Wbp * per_view * 4);
-  if (st == HR_OK) st = alloc(p, (void**)&p->d_vslab, (size_t)G.XN * G.YN * p->S * 4);
+  for (int b = 0; b < 2 && st == HR_OK; ++b) st = alloc(p, (void**)&p->d_vslab[b], (size_t)G.XN * G.YN * p->S * 4);
   if (st == HR_OK) {
     cudaError_t e = cudaStreamCreateWithFlags(&p->sc, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->scopy, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->sout, cudaStreamNonBlocking);
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
       e = cudaEventCreateWithFlags(&p->copied[b], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->consumed[b], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->computed[b], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->drained[b], cudaEventDisableTiming);
     }
     if (e != cudaSuccess) st = hr::fail(HR_ERR_CUDA, "hr_slab_plan_create: %s", cudaGetErrorString(e));
   }
@@ -205,7 +214,7 @@ static int prepare(hr_slab_plan* p, const float* fan, bool fan_on_host) {
   HR_TRY(hr::bp_fast_upload(&p->fast[k & 1], h, p->sc));
   HR_TRY(hr_rebin_execute(p->rebin, p->d_reb, p->d_fan[k & 1], p->sc));
   HR_TRY(hr_filter_tc_execute(p->ftc, p->d_pairs, p->d_reb, HR_LAYOUT_REBIN, p->margin, p->sc));
-  HR_TRY(hr::bp_fast_autotune(&p->fast[k & 1], p->gslab, p->d_vslab, p->d_pairs, p->sc));
+  HR_TRY(hr::bp_fast_autotune(&p->fast[k & 1], p->gslab, p->d_vslab[k & 1], p->d_pairs, p->sc));
   p->fast[(k & 1) ^ 1].variant = p->fast[k & 1].variant;
   p->fast[(k & 1) ^ 1].tuned = p->fast[k & 1].tuned;
   HR_TRY(hr::bp_fast_tex_prepare(&p->fast[(k & 1) ^ 1], p->gslab));
@@ -243,16 +252,22 @@ extern "C" int hr_slab_execute(hr_slab_plan* p, float* vol, const float* fan, in
     hr::BpFastHost h;
     HR_TRY(hr::bp_fast_host_tables(&h, slab_geom(p, k), p->w.data()));
     HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->copied[b], 0));
+    HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->drained[b], 0));  // slab k-2's volume has left d_vslab[b]
     HR_TRY(hr::bp_fast_upload(&p->fast[b], h, p->sc));
     HR_CUDA_TRY(cudaGraphLaunch(p->graph[b], p->sc));
     HR_CUDA_TRY(cudaEventRecord(p->consumed[b], p->sc));
+    HR_CUDA_TRY(cudaEventRecord(p->computed[b], p->sc));
     if (k + 1 < p->nslabs) HR_TRY(enqueue_fan_copy(p, k + 1, fan, fan_on_host != 0));
-    // the slab's slices are a strided block of the z-fastest volume
+    // the slab's slices are a strided block of the z-fastest volume; copied out
+    // on the output stream while the next slab computes
     const size_t ld = (size_t)G.ZN * 4;
-    HR_CUDA_TRY(cudaMemcpy2DAsync(vol + p->first_slice[k], ld, p->d_vslab, (size_t)p->S * 4,
+    HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->computed[b], 0));
+    HR_CUDA_TRY(cudaMemcpy2DAsync(vol + p->first_slice[k], ld, p->d_vslab[b], (size_t)p->S * 4,
                                   (size_t)p->n_slices[k] * 4, (size_t)G.XN * G.YN,
-                                  vol_on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, p->sc));
+                                  vol_on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, p->sout));
+    HR_CUDA_TRY(cudaEventRecord(p->drained[b], p->sout));
   }
+  HR_CUDA_TRY(cudaStreamSynchronize(p->sout));
   HR_CUDA_TRY(cudaStreamSynchronize(p->sc));
   return hr_filter_tc_check(p->ftc);
 }
