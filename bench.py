@@ -80,7 +80,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--e2e-slab", type=int, default=256,
+    ap.add_argument("--e2e-slab", type=int, default=128,
                     help="fast form: also time e2e through the slab pipeline with slabs of this many slices "
                          "(0: off); the faster entry is reported")
     return ap.parse_args()
