@@ -641,9 +641,8 @@ static int build_host(BpFastHostSet* t, int NZ, const BpFastGeom& g, const doubl
   return HR_OK;
 }
 
-int bp_fast_host_tables(BpFastHost* h, const BpFastGeom& g, const double* w, int only_nz) {
-  for (int i = 0; i < kFastTableSets; ++i)
-    if (only_nz == 0 || kFastNz[i] == only_nz) HR_TRY(build_host(&h->set[i], kFastNz[i], g, w));
+int bp_fast_host_tables(BpFastHost* h, const BpFastGeom& g, const double* w) {
+  for (int i = 0; i < kFastTableSets; ++i) HR_TRY(build_host(&h->set[i], kFastNz[i], g, w));
   h->trig.resize(g.PN);
   for (int p = 0; p < g.PN; ++p) {
     const double View = g.BetaS + p * g.DeltaFai;
@@ -675,7 +674,6 @@ int bp_fast_upload(BpFast* f, const BpFastHost& h, cudaStream_t s) {
   for (int i = 0; i < kFastTableSets; ++i) {
     BpFastTables& t = f->t[i];
     const BpFastHostSet& ht = h.set[i];
-    if (ht.nz == 0) continue;  // not built
     HR_REQUIRE(ht.nblocks == t.nblocks && ht.mask.size() <= t.cap_rows,
                "fast backprojection: tables exceed the reserved capacity");
     HR_CUDA_TRY(cudaMemcpyAsync(t.d_tab, ht.tab.data(), sizeof(float2) * ht.tab.size(), cudaMemcpyHostToDevice, s));

@@ -96,9 +96,7 @@ int bp_fast_create(BpFast* f, const BpFastGeom& g, const double* w);
 // Pieces of bp_fast_create for plans whose geometry changes between launches
 // (z slabs): build the tables of a geometry on the host, reserve device
 // capacity once, upload (stream-ordered) before each launch.
-// only_nz: build only the table set of that many slices per thread (0: all);
-// bp_fast_upload skips the sets not built.
-int bp_fast_host_tables(BpFastHost* h, const BpFastGeom& g, const double* w, int only_nz = 0);
+int bp_fast_host_tables(BpFastHost* h, const BpFastGeom& g, const double* w);
 int bp_fast_reserve(BpFast* f, const size_t rows[kFastTableSets], const int nblocks[kFastTableSets], int PN);
 int bp_fast_upload(BpFast* f, const BpFastHost& h, cudaStream_t s);
 void bp_fast_destroy(BpFast* f);

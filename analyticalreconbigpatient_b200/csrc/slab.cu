@@ -250,7 +250,7 @@ extern "C" int hr_slab_execute(hr_slab_plan* p, float* vol, const float* fan, in
     const int b = k & 1;
     // tables of slab k: host build (overlaps the previous slab on the GPU), stream-ordered upload
     hr::BpFastHost h;
-    HR_TRY(hr::bp_fast_host_tables(&h, slab_geom(p, k), p->w.data(), hr::bp_fast_variant_nz(p->fast[b].variant)));
+    HR_TRY(hr::bp_fast_host_tables(&h, slab_geom(p, k), p->w.data()));
     HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->copied[b], 0));
     HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->drained[b], 0));  // slab k-2's volume has left d_vslab[b]
     HR_TRY(hr::bp_fast_upload(&p->fast[b], h, p->sc));
