@@ -23,7 +23,9 @@
 // channels u (low half) and u+1 (high half), so one 32-bit load gives both
 // horizontal taps of a row. The bilinear tap uses floor instead of the
 // reference's ceil; both give the same interpolated value away from exact
-// integers, where the blend is continuous.
+// integers, where the blend is continuous. The texture variants (further
+// down) copy the pairs' low halves into layered FP16 or FP32 textures and let
+// the texture units do the bilinear tap.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 

@@ -183,10 +183,13 @@ int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const double* w, i
  * for HR_FORM_FAST); d_vol: device [YN][XN][ZN] (double for HR_FORM_FP64, else float). */
 int hr_bp_execute(const hr_bp_plan* plan, void* d_vol, const void* d_fp, void* stream);
 void hr_bp_plan_destroy(hr_bp_plan* plan);
-/* HR_FORM_FAST: times the kernel variants (slices per thread x gathers issued
- * together) on a 32-slice band of d_vol and keeps the fastest for the plan's
- * later executions. Synchronises the stream; call before graph capture. Other
- * forms: no-op. */
+/* HR_FORM_FAST: times the kernel variants (slices per thread x register
+ * gathers or texture-sampled taps, see hr_bp_select) on a 32-slice band of
+ * d_vol and keeps the fastest for the plan's later executions; a texture
+ * variant keeps an FP16 (2 bytes per sample) or FP32 layered copy of the
+ * filtered data in the plan, refilled by every hr_bp_execute, so two
+ * executions of one such plan must not overlap on the GPU. Synchronises the
+ * stream and may allocate; call before graph capture. Other forms: no-op. */
 int hr_bp_autotune(hr_bp_plan* plan, void* d_vol, const void* d_fp, void* stream);
 /* Writes a one-line description of the kernel configuration into buf. */
 int hr_bp_describe(const hr_bp_plan* plan, char* buf, int len);
