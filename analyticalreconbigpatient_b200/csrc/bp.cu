@@ -256,29 +256,24 @@ __global__ void __launch_bounds__(kBx* kBy) bp_fp64_kernel(double* __restrict__ 
 constexpr int kNzPlain = 8;
 constexpr int kNzFp64 = 4;
 
-}  // namespace
-
-extern "C" int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const double* w, int form) {
-  hr::clear_error();
-  HR_REQUIRE(plan != nullptr && g != nullptr && w != nullptr, "hr_bp_plan_create: NULL argument");
-  *plan = nullptr;
-  HR_REQUIRE(form == HR_FORM_PLAIN || form == HR_FORM_FP64 || form == HR_FORM_FAST,
-             "hr_bp_plan_create: unknown form %d", form);
+// Checks a backprojection geometry and fills the kernels' parameter block. Every
+// entry that backprojects (the plans and the allocation-free entry) goes through
+// it, so they accept exactly the same geometries.
+int bp_params_from_geom(const hr_bp_geom* g, const char* who, BpParams* out) {
   HR_REQUIRE(g->XN > 0 && g->YN > 0 && g->ZN > 0 && g->YL > 1 && g->ZL > 1 && g->PN > 0 && g->N_2pi > 1,
-             "backprojection: invalid sizes");
+             "%s: invalid sizes", who);
   HR_REQUIRE(g->h != 0.0 && g->DeltaFai != 0.0 && g->dYL != 0.0 && g->dZL != 0.0 && g->SO > 0.0,
-             "backprojection: h, DeltaFai, dYL, dZL must be non-zero and SO > 0");
-  HR_REQUIRE((long long)g->XN * g->YN * g->ZN < (1LL << 40), "backprojection: volume too large");
-  HR_REQUIRE(g->N_2pi <= 8192, "backprojection: N_2pi=%d exceeds 8192", g->N_2pi);
+             "%s: h, DeltaFai, dYL, dZL must be non-zero and SO > 0", who);
+  HR_REQUIRE((long long)g->XN * g->YN * g->ZN < (1LL << 40), "%s: volume too large", who);
+  HR_REQUIRE(g->N_2pi <= 8192, "%s: N_2pi=%d exceeds 8192", who, g->N_2pi);
   // For views in [s0-half, s0+half] the weight indices are d1 = N_pi-(s0-p)
   // and d1 +/- N_pi; they stay inside [0, N_2pi) iff half <= N_pi and
   // N_pi + half <= N_2pi - 1 (the reference GPU kernel reads outside it).
   const int half = (int)std::ceil(g->N_pi * g->HSCoef);
   HR_REQUIRE(half >= 0 && (double)half <= g->N_pi && g->N_pi + half <= g->N_2pi - 1 &&
                  2.0 * g->N_pi <= g->N_2pi + 1e-9,
-             "backprojection: HSCoef=%g, N_pi=%g give a view window outside the weight table", g->HSCoef, g->N_pi);
+             "%s: HSCoef=%g, N_pi=%g give a view window outside the weight table", who, g->HSCoef, g->N_pi);
   HR_TRY(hr::require_device());
-
   BpParams P{};
   P.XN = g->XN; P.YN = g->YN; P.ZN = g->ZN; P.YL = g->YL; P.ZL = g->ZL; P.PN = g->PN; P.N_2pi = g->N_2pi;
   P.half = half;
@@ -290,13 +285,34 @@ extern "C" int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const d
   P.SOSDdZL = P.SOSD / g->dZL;
   P.k1f = (float)g->k1;
   P.DeltaFaif = (float)g->DeltaFai;
+  *out = P;
+  return HR_OK;
+}
 
-  // Per-view tables in the reference's own arithmetic (:73, :76-79).
-  std::vector<ViewTab> tab(g->PN);
-  for (int p = 0; p < g->PN; ++p) {
-    const double View = g->BetaS + p * g->DeltaFai;
-    tab[p] = ViewTab{std::cos(View), std::sin(View), g->h * View * kInvTwoPi};
+// Per-view tables in the reference's own arithmetic
+// (src/Parallel_FDK_Helical_3DWeighting.cpp:73, :76-79): the host C library's
+// cos/sin, which the bit-exact index selection depends on.
+void fill_view_table(ViewTab* tab, int PN, double BetaS, double DeltaFai, double h) {
+  for (int p = 0; p < PN; ++p) {
+    const double View = BetaS + p * DeltaFai;
+    tab[p] = ViewTab{std::cos(View), std::sin(View), h * View * kInvTwoPi};
   }
+}
+
+}  // namespace
+
+extern "C" int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const double* w, int form) {
+  hr::clear_error();
+  HR_REQUIRE(plan != nullptr && g != nullptr && w != nullptr, "hr_bp_plan_create: NULL argument");
+  *plan = nullptr;
+  HR_REQUIRE(form == HR_FORM_PLAIN || form == HR_FORM_FP64 || form == HR_FORM_FAST,
+             "hr_bp_plan_create: unknown form %d", form);
+  BpParams P{};
+  HR_TRY(bp_params_from_geom(g, "backprojection", &P));
+  const int half = P.half;
+
+  std::vector<ViewTab> tab(g->PN);
+  fill_view_table(tab.data(), g->PN, g->BetaS, g->DeltaFai, g->h);
   std::vector<float> wf(g->N_2pi);
   for (int i = 0; i < g->N_2pi; ++i) wf[i] = (float)w[i];
 
@@ -401,15 +417,20 @@ extern "C" void hr_bp_plan_destroy(hr_bp_plan* pl) {
 // ---------------------------------------------------------------------------
 // Plain-form backprojection that allocates nothing.
 //
-// Some callers cannot call cudaMalloc: code that runs while its stream is being
-// captured into a CUDA graph (allocation is not allowed during capture),
-// streaming pipelines that must not allocate after start-up because
-// cudaMalloc/cudaFree synchronise the device, and hosts such as MATLAB or a
-// framework's pooling allocator that own all device memory. This entry keeps
-// its only scratch -- the per-view cos/sin/source-height table -- in a
-// file-scope device array of kNoAllocMaxViews entries (768 KiB, held by every
-// GPU that loads the library until the process exits) and takes everything
-// else (filtered data, weight table, volume) from the caller.
+// Some callers cannot call cudaMalloc: streaming pipelines that must not
+// allocate once they run, because cudaMalloc and cudaFree synchronise the whole
+// device and would stall the other streams; hosts whose pooling allocator owns
+// all device memory (a MATLAB session, a framework's caching allocator), where
+// a second allocator fragments or exhausts the pool; and services that run
+// under a fixed device-memory budget. This entry keeps its only scratch -- the
+// per-view cos/sin/source-height table -- in a file-scope device array of
+// kNoAllocMaxViews entries (768 KiB, held by every GPU that loads the library
+// until the process exits) and takes everything else (filtered data, weight
+// table, volume) from the caller.
+//
+// The table is computed on the host with the same C library calls as the plan
+// (fill_view_table) and copied into the array, so both entries select the same
+// view/row/channel indices and give bit-identical volumes.
 // ---------------------------------------------------------------------------
 #include <mutex>
 
@@ -424,15 +445,17 @@ namespace {
 
 std::mutex g_noalloc_mutex;
 ViewTab* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+// Host staging of the table (pageable, file scope: filled and copied under
+// g_noalloc_mutex).
+ViewTab g_noalloc_host[kNoAllocMaxViews];
 
 // Device address of g_noalloc_views on the current device, looked up once per
 // device (with that device current). In host code the array's name is only a
-// host-side stand-in, never a device address.
+// host-side stand-in, never a device address. Called with g_noalloc_mutex held.
 int noalloc_views(ViewTab** out) {
   int dev = 0;
   HR_CUDA_TRY(cudaGetDevice(&dev));
   HR_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, "hr_bp_plain_noalloc: device %d out of range", dev);
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   if (g_noalloc_ptr[dev] == nullptr) {
     void* p = nullptr;
     HR_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_views));
@@ -442,18 +465,6 @@ int noalloc_views(ViewTab** out) {
   return HR_OK;
 }
 
-// cos/sin/h*View/2pi of every view, with the same double expressions the plan
-// evaluates on the host (View = BetaS + p*DeltaFai, h*View*invPI).
-__global__ void noalloc_view_table_kernel(ViewTab* __restrict__ tab, int PN, double BetaS, double DeltaFai,
-                                          double h) {
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < PN; p += gridDim.x * blockDim.x) {
-    const double View = __dadd_rn(BetaS, __dmul_rn((double)p, DeltaFai));
-    double s, c;
-    sincos(View, &s, &c);
-    tab[p] = ViewTab{c, s, __dmul_rn(__dmul_rn(h, View), kInvTwoPi)};
-  }
-}
-
 }  // namespace
 
 extern "C" int hr_bp_plain_noalloc(float* d_vol, const float* d_fp, const float* d_w, const hr_bp_geom* g,
@@ -461,37 +472,23 @@ extern "C" int hr_bp_plain_noalloc(float* d_vol, const float* d_fp, const float*
   hr::clear_error();
   HR_REQUIRE(d_vol != nullptr && d_fp != nullptr && d_w != nullptr && g != nullptr,
              "hr_bp_plain_noalloc: NULL argument");
-  HR_REQUIRE(g->XN > 0 && g->YN > 0 && g->ZN > 0 && g->YL > 1 && g->ZL > 1 && g->PN > 0 && g->N_2pi > 1,
-             "hr_bp_plain_noalloc: invalid sizes");
   HR_REQUIRE(g->PN <= kNoAllocMaxViews,
              "hr_bp_plain_noalloc: PN=%d views exceed the fixed scratch table of %d views (use hr_bp_plan_create)",
              g->PN, kNoAllocMaxViews);
-  HR_REQUIRE(g->N_2pi <= 8192, "hr_bp_plain_noalloc: N_2pi=%d exceeds 8192", g->N_2pi);
-  HR_REQUIRE(g->h != 0.0 && g->DeltaFai != 0.0 && g->dYL != 0.0 && g->dZL != 0.0 && g->SO > 0.0,
-             "hr_bp_plain_noalloc: h, DeltaFai, dYL, dZL must be non-zero and SO > 0");
-  const int half = (int)std::ceil(g->N_pi * g->HSCoef);
-  HR_REQUIRE(half >= 0 && (double)half <= g->N_pi && g->N_pi + half <= g->N_2pi - 1 &&
-                 2.0 * g->N_pi <= g->N_2pi + 1e-9,
-             "hr_bp_plain_noalloc: HSCoef=%g, N_pi=%g give a view window outside the weight table", g->HSCoef,
-             g->N_pi);
   BpParams P{};
-  P.XN = g->XN; P.YN = g->YN; P.ZN = g->ZN; P.YL = g->YL; P.ZL = g->ZL; P.PN = g->PN; P.N_2pi = g->N_2pi;
-  P.half = half;
-  P.XNC = g->XNC; P.YNC = g->YNC; P.ZNC = g->ZNC; P.dx = g->dx; P.dy = g->dy; P.dz = g->dz;
-  P.YLC = g->YLC; P.ZLC = g->ZLC; P.dYL = g->dYL; P.dZL = g->dZL; P.h = g->h; P.BetaS = g->BetaS;
-  P.DeltaFai = g->DeltaFai; P.N_pi = g->N_pi; P.SO = g->SO; P.SD = g->SD; P.k1 = g->k1;
-  P.SO2 = g->SO * g->SO;
-  P.SOSD = g->SO * g->SD;
-  P.SOSDdZL = P.SOSD / g->dZL;
-  P.k1f = (float)g->k1;
-  P.DeltaFaif = (float)g->DeltaFai;
+  HR_TRY(bp_params_from_geom(g, "hr_bp_plain_noalloc", &P));
   dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, (P.ZN + kNzPlain - 1) / kNzPlain);
   HR_REQUIRE(grid.z <= 65535 && grid.y <= 65535, "hr_bp_plain_noalloc: grid too large");
-  ViewTab* views = nullptr;
-  HR_TRY(noalloc_views(&views));
   cudaStream_t s = hr::as_stream(stream);
-  noalloc_view_table_kernel<<<(P.PN + 255) / 256, 256, 0, s>>>(views, P.PN, P.BetaS, P.DeltaFai, P.h);
-  HR_CUDA_TRY(cudaGetLastError());
+  ViewTab* views = nullptr;
+  {
+    // A copy from pageable host memory returns once the data are staged, so
+    // the host buffer may be refilled by the next call as soon as it returns.
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    HR_TRY(noalloc_views(&views));
+    fill_view_table(g_noalloc_host, P.PN, P.BetaS, P.DeltaFai, P.h);
+    HR_CUDA_TRY(cudaMemcpyAsync(views, g_noalloc_host, sizeof(ViewTab) * P.PN, cudaMemcpyHostToDevice, s));
+  }
   bp_plain_kernel<kNzPlain><<<grid, dim3(kBx, kBy), sizeof(float) * P.N_2pi, s>>>(d_vol, d_fp, views, d_w, P);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;

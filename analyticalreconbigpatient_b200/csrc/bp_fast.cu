@@ -403,8 +403,11 @@ __global__ void __launch_bounds__(kBx* kBy, MB) bp_fast_batch_kernel(const __gri
 // The hardware blends with 1.8 fixed-point weights, so a tap differs from the
 // FP32 blend by up to 1/256 of the neighbour difference (the fast form's
 // accuracy budget covers it). Taps come from the low halves of the BF16 pairs:
-// the same sample values as the gather variants (FP16 holds every BF16 value
-// of the scaled range exactly).
+// the same sample values as the gather variants wherever FP16 holds the BF16
+// value exactly. The scale puts the largest |value| in [2^14, 2^15), and FP16
+// (subnormals included) represents a BF16 value exactly down to 2^-17, i.e.
+// over 2^31 below the largest |value|; smaller values are rounded to FP16's
+// 2^-24 step (an absolute error of at most 2^-39 of the largest |value|).
 
 // Largest |value| of the filtered data (bits of a non-negative float order
 // like unsigned integers), for the FP16 scale.

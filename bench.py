@@ -79,7 +79,7 @@ def parse():
                          "timed beside it unless --no-plain")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--e2e-slab", type=int, default=128,
                     help="fast form: also time e2e through the slab pipeline with slabs of this many slices "
                          "(0: off); the faster entry is reported")
@@ -189,13 +189,15 @@ def cpu_baseline(scan, budget_s: float = 20.0, kind: str = "auto"):
     t = time.perf_counter()
     with ThreadPoolExecutor(ncores) as ex:
         list(ex.map(lambda b: fn(b, **a), blocks))
-    t_rebin = (time.perf_counter() - t) * ra["ViewN"] / (ncores * (nv + 160))
+    t_rebin_sample = time.perf_counter() - t
+    t_rebin = t_rebin_sample * ra["ViewN"] / (ncores * (nv + 160))
     # filter: rows of a block of views (OpenMP inside)
     nvf = max(1, min(200, fa["ViewN"]))
     rows = rng.standard_normal((nvf, fa["ZL"], fa["YL"]))
     t = time.perf_counter()
     oracle.filter_f64(rows, **dict(fa, ViewN=nvf), nthreads=ncores)
-    t_filter = (time.perf_counter() - t) * fa["ViewN"] / nvf
+    t_filter_sample = time.perf_counter() - t
+    t_filter = t_filter_sample * fa["ViewN"] / nvf
     # backprojection: whole slices of a z band in the middle of the scan, split by y rows
     w = oracle.weight_table(scan.N_2pi, scan.HSCoef, scan.delta)
     nz = 2
@@ -222,13 +224,15 @@ def cpu_baseline(scan, budget_s: float = 20.0, kind: str = "auto"):
         list(ex.map(lambda gg: bp_fn(fp, w, gg), subs))
     t_bp_sample = time.perf_counter() - t
     upd_sample = ncores * ny_per_thread * g["XN"] * nz * 671
+    timed_s = t_rebin_sample + t_filter_sample + t_bp_sample
     t_bp = t_bp_sample * scan.updates() / upd_sample
     total = t_rebin + t_filter + t_bp
     detail = {"rebin_s": t_rebin, "filter_s": t_filter, "bp_s": t_bp,
               "sample": (f"rebin {ncores}x{nv + 160} views, filter {nvf} views x {fa['ZL']} rows, backprojection "
                          f"{ncores}x{ny_per_thread} rows x {g['XN']} x {nz} slices (centre of the scan, "
                          f"{upd_sample:.3g} updates); each extrapolated linearly to the full volume"),
-              "kind": "reference" if use_ref else "port", "cores": ncores}
+              "kind": "reference" if use_ref else "port", "cores": ncores,
+              "sample_updates": upd_sample, "sample_wall_s": timed_s}
     return scan.updates() / total / 1e9, total, detail
 
 
@@ -240,19 +244,32 @@ def run_reference(args, scan, rank, world):
     for i in range(args.warmup + args.steps):
         gups, spv, detail = cpu_baseline(scan, budget_s=8.0)
         if i >= args.warmup:
-            steps.append((gups, spv))
+            steps.append((gups, spv, detail["sample_wall_s"]))
     gups = statistics.median(s[0] for s in steps)
     spv = statistics.median(s[1] for s in steps)
     line = {"impl": "reference", "metric": "GUPS (voxel-view updates/s, rebin+filter+3D-weighted helical BP)",
             "value": gups, "unit": "GUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": spv * 1e3, "s_per_volume": spv, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": scan_name(scan, args.config), "flush": "n/a (CPU)"},
+            "config": chain_config(scan, args.config, world),
+            "extrapolated": True,
+            "timed_sample": {"updates_per_step": detail["sample_updates"],
+                             "wall_s_per_step": statistics.median(s[2] for s in steps),
+                             "note": "each step times a bounded sample of every stage on the host cores and "
+                                     "extrapolates it linearly to the whole volume; ms_per_step is that "
+                                     "extrapolation, not a timed interval"},
             "cpu_baseline": {"value": gups, "unit": "GUPS", "cores": detail["cores"], "kind": detail["kind"],
                              "sample": detail["sample"]},
             "e2e": {"value": gups, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "detail": {k: detail[k] for k in ("rebin_s", "filter_s", "bp_s")}}
     print(json.dumps(line), flush=True)
+
+
+def chain_config(scan, config, world):
+    """The `config` object of the chain's line; the reference arm prints the same one."""
+    return {"workload": scan_name(scan, config), "updates_per_volume": scan.updates(),
+            "parallelism": f"independent scans x{world}" if world > 1 else "1 GPU",
+            "flush": "inputs larger than L2 (fan data 4.47 GB, filtered data 4.4 GB)"}
 
 
 def scan_name(scan, config):
@@ -825,9 +842,7 @@ def main():
             "dtype": "bf16" if chosen == _lib.HR_FORM_FAST else "f32",
             "data": "synthetic (analytic FP64 projections of seeded random-ellipsoid phantoms)",
             "form": args.form,
-            "config": {"workload": scan_name(scan, args.config), "updates_per_volume": updates,
-                       "parallelism": f"independent scans x{world}" if world > 1 else "1 GPU",
-                       "flush": "inputs larger than L2 (fan data 4.47 GB, filtered data 4.4 GB)"},
+            "config": chain_config(scan, args.config, world),
             "stages_ms": res["stages_ms"],
             "roofline": roofline,
             "e2e": {"value": e2e_value, "unit": "GUPS", "s_per_volume": res["e2e_s"],
@@ -844,7 +859,8 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         gups, spv, detail = cpu_baseline(scan)
         line["cpu_baseline"] = {"value": gups, "unit": "GUPS", "cores": detail["cores"], "kind": detail["kind"],
-                                "sample": detail["sample"], "s_per_volume": spv}
+                                "sample": detail["sample"], "s_per_volume": spv, "extrapolated": True,
+                                "sample_updates": detail["sample_updates"], "sample_wall_s": detail["sample_wall_s"]}
         # beside it, a straight CPU build of the same formulas (the C restatement in oracle/)
         gups_p, spv_p, detail_p = cpu_baseline(scan, budget_s=10.0, kind="port")
         line["cpu_port"] = {"value": gups_p, "unit": "GUPS", "cores": detail_p["cores"], "kind": "port",

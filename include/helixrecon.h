@@ -50,7 +50,7 @@ void ParallelRebinningCBCurve_GPU(float* outputProj, const float* Proj, const in
 void filtering(float* hfpwd, const float* hProj, const int YL, const int ZL, const int ViewN, const float PLC,
                const float ZLC, const float dYL, const float dZL, const float SO);
 
-/* Replaces src/ParallelFDKHelical3DWeightingGPU.h:4-13 / ...GPU.cu:421-436.
+/* Replaces src/ParallelFDKHelical3DWeightingGPU.h:4-13 / ...GPU.cu:125-140.
  * FP64 data path on the GPU; views s1..s2 as the reference's CPU loop. */
 void ParallekFDKHelical3DWeighting_GPU_double(
     double* hctimage, const double* hfp, const double* hw, const int N_2pi, const int XN, const int YN,
@@ -59,7 +59,7 @@ void ParallekFDKHelical3DWeighting_GPU_double(
     const double dYL, const double dZL, const double h, const double BetaS, const double DeltaFai,
     const double N_pi, const double HSCoef, const double SO, const double SD, const double k1);
 
-/* Replaces src/ParallelFDKHelical3DWeightingGPU.h:15-24 / ...GPU.cu:440-455.
+/* Replaces src/ParallelFDKHelical3DWeightingGPU.h:15-24 / ...GPU.cu:144-159.
  * FP32 data path; view/row/channel index selection computed in FP64 with the
  * reference CPU's expression order, so it is bit-exact to that path. */
 void ParallekFDKHelical3DWeighting_GPU_float(
@@ -206,16 +206,19 @@ int hr_bp_select(hr_bp_plan* plan, int variant);
 
 /* ---- backprojection that allocates nothing ------------------------------ */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc:
- * code running while its stream is captured into a CUDA graph, streaming
- * pipelines that may not allocate after start-up (cudaMalloc/cudaFree
- * synchronise the device), and hosts whose pooling allocator owns all device
- * memory. Same result as a HR_FORM_PLAIN plan: d_vol [YN][XN][ZN] float,
- * d_fp [PN][ZL][YL] float, d_w the N_2pi view weights as float on the device.
- * Its per-view table lives in a fixed device array inside the library, so
- * PN is limited to 32768 views (HR_ERR_INVALID_ARGUMENT beyond). The first
- * call on a device looks up that array's address (cudaGetSymbolAddress) and
- * should come before any stream capture. All calls share the array: calls
- * that overlap on the GPU (other streams, other threads) race. */
+ * streaming pipelines that must not allocate once running (cudaMalloc and
+ * cudaFree synchronise the whole device), hosts whose pooling allocator owns
+ * all device memory (a MATLAB session, a framework's caching allocator), and
+ * services held to a fixed device-memory budget. Same result, bit for bit, as
+ * a HR_FORM_PLAIN plan: d_vol [YN][XN][ZN] float, d_fp [PN][ZL][YL] float,
+ * d_w the N_2pi view weights as float on the device; the geometry checks are
+ * the plan's. Its per-view table is computed on the host with the plan's C
+ * library calls and copied (from pageable memory, so the call first waits for
+ * the stream's earlier work) into a fixed 768 KiB device array inside the
+ * library: PN is limited to 32768 views (HR_ERR_INVALID_ARGUMENT beyond). The
+ * first call on a device looks up that array's address (cudaGetSymbolAddress).
+ * All calls share the array and it keeps the last call's table: calls that
+ * overlap on the GPU (other streams, other threads) race. */
 int hr_bp_plain_noalloc(float* d_vol, const float* d_fp, const float* d_w, const hr_bp_geom* g, void* stream);
 
 /* ---- BF16 channel pairs (the fast form's filtered-data layout) ---------- */

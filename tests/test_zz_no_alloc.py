@@ -1,13 +1,15 @@
 """The allocation-free backprojection entry (hr_bp_plain_noalloc).
 
-It exists for callers that cannot call cudaMalloc -- code running under CUDA
-graph capture, streaming pipelines that must not allocate (cudaMalloc and
-cudaFree synchronise the device), hosts whose allocator owns all device
-memory. Its scratch (the per-view table) is a fixed array inside the library.
-The test calls it through the C ABI twice in a row, on two different scans,
-and checks each result against the plan-based plain entry (hr_bp_execute)
-within the plain form's tolerance. This file sorts last so that a run stopping
-at the first failure has run every other test first.
+It exists for callers that cannot call cudaMalloc: pipelines that must not
+allocate once running (cudaMalloc and cudaFree synchronise the device), hosts
+whose pooling allocator owns all device memory, services held to a fixed
+memory budget. Its scratch (the per-view table) is a fixed array inside the
+library, filled from the same host-computed table as the plan's. The tests call
+it through the C ABI twice in a row, on two different scans, and on a scan of
+nearly the array's maximum number of views, and require the volume to equal the
+plan-based plain entry's (hr_bp_execute) bit for bit (the plain form's index
+selection is exact, so no tolerance is needed). This file sorts last so that a
+run stopping at the first failure has run every other test first.
 """
 import ctypes
 
@@ -42,22 +44,40 @@ def _plan_result(geom, w, fp, shape, dev):
     return vol.cpu().numpy()
 
 
-def test_no_alloc_entry_matches_plan_entry_on_two_calls(cuda):
+def _noalloc_result(geom, w, fp, shape, dev):
     lib = _lib.load()
+    d_w = torch.tensor(w.astype(np.float32), device=dev)
+    vol = torch.full(shape, float("nan"), dtype=torch.float32, device=dev)
+    _lib.check(lib.hr_bp_plain_noalloc(vol.data_ptr(), fp.data_ptr(), d_w.data_ptr(), ctypes.byref(geom), 0))
+    torch.cuda.synchronize()
+    return vol.cpu().numpy()
+
+
+def test_no_alloc_entry_matches_plan_entry_on_two_calls(cuda):
     scans = [G.Scan(ZL=16, pitch=0.9375, rotations=3, XN=48, YN=40, ZN=20, dx=5.0, dy=5.5, dz=1.0),
              G.Scan(ZL=8, pitch=1.2, rotations=2.5, XN=32, YN=36, ZN=13, dx=6.0, dy=6.0, dz=2.0, beta_start=40.0,
                     delta=40)]
     for seed, sc in enumerate(scans):
         geom, w, fp = _case(sc, seed, cuda)
-        d_w = torch.tensor(w.astype(np.float32), device=cuda)
-        vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), dtype=torch.float32, device=cuda)
-        _lib.check(lib.hr_bp_plain_noalloc(vol.data_ptr(), fp.data_ptr(), d_w.data_ptr(), ctypes.byref(geom), 0))
-        torch.cuda.synchronize()
-        mine = vol.cpu().numpy()
-        ref = _plan_result(geom, w, fp, (sc.YN, sc.XN, sc.ZN), cuda)
+        shape = (sc.YN, sc.XN, sc.ZN)
+        mine = _noalloc_result(geom, w, fp, shape, cuda)
+        ref = _plan_result(geom, w, fp, shape, cuda)
         assert np.isfinite(mine).all()
         assert rel_l2(mine, ref) < PLAIN_TOL, seed
-        assert np.array_equal(mine == 0, ref == 0)
+        assert np.array_equal(mine, ref), (seed, int(np.sum(mine != ref)))
+
+
+def test_no_alloc_entry_bit_exact_on_many_views(cuda):
+    # 30 rotations: 29,520 fan views (near the 32,768-view limit), source angles
+    # up to ~95 rad, slices spread over the whole helix
+    sc = G.Scan(ZL=16, pitch=0.9375, rotations=30, XN=24, YN=24, ZN=28, dx=12.0, dy=12.0, dz=9.5)
+    geom, w, fp = _case(sc, 7, cuda)
+    assert sc.PN > 29000
+    shape = (sc.YN, sc.XN, sc.ZN)
+    mine = _noalloc_result(geom, w, fp, shape, cuda)
+    ref = _plan_result(geom, w, fp, shape, cuda)
+    assert np.count_nonzero(ref) > ref.size // 2
+    assert np.array_equal(mine, ref), int(np.sum(mine != ref))
 
 
 def test_no_alloc_entry_rejects_too_many_views(cuda):
