@@ -15,6 +15,7 @@ HR_OK = 0
 HR_ERR_INVALID_ARGUMENT, HR_ERR_CUDA, HR_ERR_OUT_OF_MEMORY, HR_ERR_NO_DEVICE, HR_ERR_UNSUPPORTED = 1, 2, 3, 4, 5
 HR_FORM_PLAIN, HR_FORM_FP64, HR_FORM_FAST = 0, 1, 2
 HR_LAYOUT_ROWS, HR_LAYOUT_REBIN = 0, 1
+HR_SLAB_BLOCKS, HR_SLAB_ROUND_ROBIN = 0, 1
 
 _i = ctypes.c_int
 _f = ctypes.c_float
@@ -45,6 +46,11 @@ class ReconDesc(ctypes.Structure):
                 + [(n, _f) for n in ("YLC", "dYA", "DeltaTheta", "PLC", "DeltaT", "DeltaFai", "SO")]
                 + [("view0", _i)] + [(n, _f) for n in ("fPLC", "fZLC", "fdYL", "fdZL", "fSO")]
                 + [("bp", BpGeom), ("w", _p), ("form", _i)])
+
+
+class SlabWindow(ctypes.Structure):
+    _fields_ = [(n, _i) for n in ("slab", "first_slice", "n_slices", "bp_view0", "bp_views", "fan_view0", "fan_views",
+                                  "shared_views")]
 
 
 class GeHeader(ctypes.Structure):
@@ -98,6 +104,10 @@ _SIGS = {
     "hr_slab_describe": (_i, [_p, ctypes.c_char_p, _i]),
     "hr_slab_device_bytes": (ctypes.c_size_t, [_p]),
     "hr_slab_plan_destroy": (None, [_p]),
+    "hr_slab_windows": (_i, [ctypes.POINTER(ReconDesc), _i, _i, _i, _i, _p, _i, ctypes.POINTER(_i)]),
+    "hr_slab_plan_create_part": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc), _i, _i, _i, _i]),
+    "hr_slab_execute_range": (_i, [_p, _p, _p, _i, _i, _i]),
+    "hr_slab_fan_range": (_i, [_p, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_size_t)]),
     "hr_recon_describe": (_i, [_p, ctypes.c_char_p, _i]),
     "hr_bp_autotune": (_i, [_p, _p, _p, _p]),
     "hr_bp_describe": (_i, [_p, ctypes.c_char_p, _i]),

@@ -105,28 +105,94 @@ class HelicalRecon:
             pass
 
 
+def slab_windows(scan: Scan, slab_slices: int, part: int = 0, nparts: int = 1,
+                 assign: int = _lib.HR_SLAB_BLOCKS) -> list[dict]:
+    """Slab windows of part ``part`` of ``nparts`` (hr_slab_windows: host
+    arithmetic only, no GPU needed): one dict per slab with its slices, its
+    backprojection window (cropped, rebinned view numbering) and its fan window."""
+    w = view_weights(scan)
+    desc = recon_desc(scan, w, _lib.HR_FORM_FAST)
+    lib = _lib.load()
+    n = ctypes.c_int(0)
+    _lib.check(lib.hr_slab_windows(ctypes.byref(desc), slab_slices, part, nparts, assign, None, 0, ctypes.byref(n)))
+    arr = (_lib.SlabWindow * max(1, n.value))()
+    _lib.check(lib.hr_slab_windows(ctypes.byref(desc), slab_slices, part, nparts, assign, arr, n.value,
+                                   ctypes.byref(n)))
+    return [{k: getattr(arr[i], k) for k, _ in _lib.SlabWindow._fields_} for i in range(n.value)]
+
+
+def plain_slab(scan: Scan, win: dict, fan_window: torch.Tensor) -> torch.Tensor:
+    """The plain FP32 chain (the drop-in numerics) on one slab of a long scan:
+    the slab's fan window ``fan_window`` [fan_views][YL][ZL] (on the device) is
+    rebinned with the whole scan's rebinning arguments, its backprojection
+    window filtered and backprojected into the slab's slices. Returns the slab
+    [YN][XN][n_slices]. The reference the slab pipeline's per-slab error is
+    stated against."""
+    lib = _lib.load()
+    ra, fa = scan.rebin_args(), scan.filter_args()
+    g = scan.bp_geom()
+    gs = dict(g, ZN=win["n_slices"], ZNC=g["ZNC"] - win["first_slice"], PN=win["bp_views"],
+              BetaS=g["BetaS"] + win["bp_view0"] * g["DeltaFai"])
+    dev = fan_window.device
+    reb, filt, bp = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    w = view_weights(scan)
+    geom = _lib.BpGeom.from_dict(gs)
+    try:
+        _lib.check(lib.hr_rebin_plan_create(ctypes.byref(reb), ra["YL"], ra["ZL"], win["fan_views"], ra["YLC"],
+                                            ra["dYA"], ra["DeltaTheta"], ra["PLC"], ra["DeltaT"], ra["DeltaFai"],
+                                            ra["SO"]))
+        _lib.check(lib.hr_filter_plan_create(ctypes.byref(filt), fa["YL"], fa["ZL"], win["bp_views"], fa["PLC"],
+                                             fa["ZLC"], fa["dYL"], fa["dZL"], fa["SO"]))
+        _lib.check(lib.hr_bp_plan_create(ctypes.byref(bp), ctypes.byref(geom), w.ctypes.data, _lib.HR_FORM_PLAIN))
+        rebinned = torch.empty_like(fan_window)
+        filtered = torch.empty((win["bp_views"], scan.ZL, scan.YL), dtype=torch.float32, device=dev)
+        out = torch.empty((scan.YN, scan.XN, win["n_slices"]), dtype=torch.float32, device=dev)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(lib.hr_rebin_execute(reb, rebinned.data_ptr(), fan_window.data_ptr(), st))
+        _lib.check(lib.hr_filter_execute(filt, filtered.data_ptr(), rebinned.data_ptr(), _lib.HR_LAYOUT_REBIN,
+                                         scan.crop_front, st))
+        _lib.check(lib.hr_bp_execute(bp, out.data_ptr(), filtered.data_ptr(), st))
+        torch.cuda.synchronize(dev)
+    finally:
+        lib.hr_rebin_plan_destroy(reb)
+        lib.hr_filter_plan_destroy(filt)
+        lib.hr_bp_plan_destroy(bp)
+    return out
+
+
 class SlabRecon:
     """Long scans reconstructed slab by slab (disjoint z slabs, each from its own
     view window) through a captured CUDA graph; see hr_slab_plan in
-    include/helixrecon.h. Fast form only."""
+    include/helixrecon.h. Fast form only. ``part``/``nparts`` split the slabs
+    of one scan between GPUs (one plan per GPU, no exchange)."""
 
-    def __init__(self, scan: Scan, slab_slices: int = 64, device: int | torch.device = 0):
+    def __init__(self, scan: Scan, slab_slices: int = 64, device: int | torch.device = 0, part: int = 0,
+                 nparts: int = 1, assign: int = _lib.HR_SLAB_BLOCKS):
         self.scan = scan
         self.device = torch.device("cuda", device) if isinstance(device, int) else device
         self._plan = ctypes.c_void_p()
         w = view_weights(scan)
         desc = recon_desc(scan, w, _lib.HR_FORM_FAST)
         with torch.cuda.device(self.device):
-            _lib.check(_lib.load().hr_slab_plan_create(ctypes.byref(self._plan), ctypes.byref(desc), slab_slices))
+            _lib.check(_lib.load().hr_slab_plan_create_part(ctypes.byref(self._plan), ctypes.byref(desc), slab_slices,
+                                                            part, nparts, assign))
 
-    def run(self, fan, volume) -> None:
-        """fan/volume: torch tensors (CUDA or CPU; pinned CPU tensors overlap copies with compute)."""
+    def fan_range(self) -> tuple[int, int, int]:
+        """(first fan view, view count, bytes copied from the fan per run)."""
+        first, n, nbytes = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_size_t(0)
+        _lib.check(_lib.load().hr_slab_fan_range(self._plan, ctypes.byref(first), ctypes.byref(n),
+                                                 ctypes.byref(nbytes)))
+        return first.value, n.value, nbytes.value
+
+    def run(self, fan, volume, fan_view0: int = 0) -> None:
+        """fan/volume: torch tensors (CUDA or CPU; pinned CPU tensors overlap copies with compute).
+        ``fan`` holds fan views [fan_view0, ...) of the scan (at least the plan's fan_range)."""
         def ptr(t):
             return (t.data_ptr(), 0) if t.is_cuda else (t.data_ptr(), 1)
         fp, fh = ptr(fan)
         vp, vh = ptr(volume)
         with torch.cuda.device(self.device):
-            _lib.check(_lib.load().hr_slab_execute(self._plan, vp, fp, vh, fh))
+            _lib.check(_lib.load().hr_slab_execute_range(self._plan, vp, fp, fan_view0, vh, fh))
 
     def describe(self) -> str:
         buf = ctypes.create_string_buffer(768)

@@ -56,9 +56,23 @@ def max_over_ranks(values, world: int, device):
     return [float(v) for v in t.tolist()]
 
 
+def sum_over_ranks(values, world: int, device):
+    """Element-wise sum over the ranks of a job (byte counts of the ranks' copies)."""
+    values = [float(v) for v in values]
+    if world <= 1:
+        return values
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()]
+
+
 def job_gups(updates_per_rank: int, world: int, seconds: float) -> float:
     """Whole-job throughput: every rank reconstructs its own scan of the same size (weak scaling)."""
     return updates_per_rank * world / seconds / 1e9
+PLAIN_LAUNCHES = 3  # plain chain: rebin, preweight + FFT filter, backprojection
 BYTES_PER_UPDATE_FP32 = 16  # four FP32 taps per voxel-view update
 BYTES_PER_UPDATE_BF16 = 8   # four BF16 taps per voxel-view update
 
@@ -79,6 +93,10 @@ def parse():
                          "timed beside it unless --no-plain")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="full config on 1 GPU: skip the big-patient, batch and learned workloads that the line "
+                         "otherwise carries as sub-objects")
+    ap.add_argument("--extra-steps", type=int, default=5, help="timed steps of each sub-workload")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--e2e-slab", type=int, default=128,
                     help="fast form: also time e2e through the slab pipeline with slabs of this many slices "
@@ -341,7 +359,8 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
     (ms,) = max_over_ranks([ms], world, dev)
     rec.check()
     out = {"ms_per_step": ms, "stages_ms": {k: statistics.mean(v) for k, v in stage_ms.items() if v},
-           "launches_per_step": 4 if fast else 3, "kernels": rec.describe()}
+           "launches_per_step": (3 + fast_launches_per_bp(rec.describe())) if fast else PLAIN_LAUNCHES,
+           "kernels": rec.describe()}
 
     # ---- end to end through the C ABI host entry -----------------------------
     if with_e2e:
@@ -388,24 +407,40 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
     return out
 
 
-def run_bigpatient(args, scan, dev, world, rank, barrier):
-    """Long scan through the slab pipeline (SlabRecon): fan data resident in HBM
-    for `value`, host-resident for `e2e`."""
-    import torch
-    import torch.distributed as dist
+def fast_launches_per_bp(desc: str) -> int:
+    """Kernels one fast-form backprojection launches: the backprojection, plus the
+    absmax and fill passes of an FP16 texture copy (the fill alone for FP32)."""
+    if "texture-fp16" in desc:
+        return 3
+    if "texture-fp32" in desc:
+        return 2
+    return 1
 
-    from analyticalreconbigpatient_b200 import phantom as P
-    from analyticalreconbigpatient_b200.pipeline import SlabRecon, project
+
+def run_bigpatient(args, scan, dev, world, rank, barrier, emit=True):
+    """Long scan through the slab pipeline (SlabRecon): fan data resident in HBM
+    for `value`, host-resident for `e2e`. With several ranks the scan's z slabs
+    are split between them in contiguous blocks (hr_slab_plan_create_part); each
+    rank holds, projects and copies only its own fan views and writes only its
+    own slices: no data cross between ranks (strong scaling: one scan)."""
+    import torch
+
+    from analyticalreconbigpatient_b200 import _lib, geometry as G, phantom as P
+    from analyticalreconbigpatient_b200.pipeline import SlabRecon, plain_slab, project, slab_windows
 
     zlo = scan.h * scan.BetaS / (2 * np.pi)
     zhi = scan.h * (scan.BetaS + scan.views * scan.dBeta) / (2 * np.pi)
     body_half = 0.5 * (zhi - zlo) + 200.0
-    objs = P.random_ellipsoids(3000 + rank, 400, (zlo, zhi), body=(250.0, 175.0), body_half_length=body_half)
-    fan = project(scan, objs, device=dev.index)
+    objs = P.random_ellipsoids(3000, 400, (zlo, zhi), body=(250.0, 175.0), body_half_length=body_half)
+    rec = SlabRecon(scan, slab_slices=args.slab, device=dev, part=rank, nparts=world, assign=_lib.HR_SLAB_BLOCKS)
+    f0, nviews, fan_bytes = rec.fan_range()
+    # this rank's fan views only: the projection of views [f0, f0 + nviews) of the scan
+    sub = G.replace(scan, beta_start=scan.BetaS + f0 * scan.dBeta, rotations=nviews / scan.N_2pi)
+    assert sub.views == nviews
+    fan = project(sub, objs, device=dev.index)
     vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, device=dev)
-    rec = SlabRecon(scan, slab_slices=args.slab, device=dev)
     for _ in range(args.warmup):
-        rec.run(fan, vol)
+        rec.run(fan, vol, fan_view0=f0)
     torch.cuda.synchronize()
     barrier()
     clocks = ClockSampler(None)
@@ -414,7 +449,7 @@ def run_bigpatient(args, scan, dev, world, rank, barrier):
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     for _ in range(args.steps):
-        rec.run(fan, vol)  # synchronous: the slab streams are drained when it returns
+        rec.run(fan, vol, fan_view0=f0)  # synchronous: the slab streams are drained when it returns
     t1.record(stream)
     torch.cuda.synchronize()
     clocks.stop()
@@ -422,7 +457,19 @@ def run_bigpatient(args, scan, dev, world, rank, barrier):
     (ms,) = max_over_ranks([ms], world, dev)
     desc = rec.describe()
     updates = scan.updates()
-    # e2e from host memory (pinned if the host allows it)
+    wins = slab_windows(scan, args.slab, rank, world, _lib.HR_SLAB_BLOCKS)
+    # per-slab error: the rank's first, middle and last slab against the plain FP32 chain on the same window
+    per_slab = []
+    for win in (wins[0], wins[len(wins) // 2], wins[-1]):
+        a = win["fan_view0"] - f0
+        ref = plain_slab(scan, win, fan[a: a + win["fan_views"]])
+        got = vol[:, :, win["first_slice"]: win["first_slice"] + win["n_slices"]]
+        hu = float(torch.sqrt(torch.mean((got.double() - ref.double()) ** 2))) / G.MU_WATER * 1000.0
+        per_slab.append({"slab": win["slab"], "slices": [win["first_slice"], win["first_slice"] + win["n_slices"]],
+                         "hu_rmse_vs_plain": hu})
+        del ref
+    torch.cuda.empty_cache()
+    # e2e from host memory (pinned if the host allows it): this rank's fan views in, its slices out
     try:
         h_fan = torch.empty(fan.shape, dtype=torch.float32, pin_memory=True)
         pinned = True
@@ -431,15 +478,19 @@ def run_bigpatient(args, scan, dev, world, rank, barrier):
         pinned = False
     h_fan.copy_(fan)
     del fan
+    torch.cuda.empty_cache()
     h_vol = torch.empty((scan.YN, scan.XN, scan.ZN), dtype=torch.float32, pin_memory=pinned)
-    rec.run(h_fan, h_vol)
+    rec.run(h_fan, h_vol, fan_view0=f0)
+    barrier()
     e2e_t = []
     for _ in range(max(1, args.e2e_steps)):
         t = time.perf_counter()
-        rec.run(h_fan, h_vol)
+        rec.run(h_fan, h_vol, fan_view0=f0)
         e2e_t.append(time.perf_counter() - t)
     (e2e_s,) = max_over_ranks([statistics.median(e2e_t)], world, dev)
     rec.close()
+    my_slices = sum(w["n_slices"] for w in wins)
+    h2d, d2h = (float(x) for x in sum_over_ranks([fan_bytes, my_slices * scan.XN * scan.YN * 4], world, dev))
     # backprojection roofline from the autotuner's best measured time per slice (same process)
     import re
 
@@ -450,30 +501,38 @@ def run_bigpatient(args, scan, dev, world, rank, barrier):
     if bp_ms_per_slice:
         upd_per_slice = updates / scan.ZN
         ach = BYTES_PER_UPDATE_BF16 * upd_per_slice / (bp_ms_per_slice * 1e-3) / 1e9
-        roof = {"bound": "hbm", "kernel": "bp_fast_kernel", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
+        roof = {"bound": "hbm", "kernel": "bp_tex_kernel" if "texture" in desc else "bp_fast_kernel",
+                "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": ach / pk["hbm_gbs"], "peak_source": pk_kind, "traffic": None,
                 "note": "gather-equivalent (8 B/update) over the autotuner's best time per slice"}
+    nslabs = len(wins)
     line = {"metric": "GUPS (voxel-view updates/s, rebin+filter+3D-weighted helical BP)",
-            "value": updates * world / (ms * 1e-3) / 1e9, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
+            "value": updates / (ms * 1e-3) / 1e9, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "s_per_volume": ms * 1e-3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "bf16",
             "data": "synthetic (analytic FP64 projections of 400 seeded random ellipsoids in a body cylinder)",
             "form": "fast (slab pipeline)",
             "config": {"workload": scan_name(scan, "bigpatient") + f", z slabs of {args.slab}",
-                       "updates_per_volume": updates, "flush": "inputs larger than L2 (44.7 GB of fan data)"},
+                       "updates_per_volume": updates,
+                       "parallelism": (f"one scan, z slabs split in blocks over {world} GPUs (no exchange)"
+                                       if world > 1 else "1 GPU"),
+                       "flush": "inputs larger than L2 (44.7 GB of fan data)"},
             "roofline": roof,
-            "e2e": {"value": updates * world / e2e_s / 1e9, "unit": "GUPS", "s_per_volume": e2e_s,
-                    "h2d_bytes_per_step": scan.projection_bytes(), "d2h_bytes_per_step": scan.volume_bytes(),
+            "e2e": {"value": updates / e2e_s / 1e9, "unit": "GUPS", "s_per_volume": e2e_s,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "host_memory": "pinned" if pinned else "pageable",
-                    "entry": "hr_slab_execute (C ABI, host buffers)"},
-            # per slab: rebin, split, Toeplitz GEMM, backprojection
-            "gpu_launches": 4 * ((scan.ZN + args.slab - 1) // args.slab) * args.steps,
+                    "entry": "hr_slab_execute_range (C ABI, host buffers; views shared by consecutive slabs "
+                             "are copied once)"},
+            "hu_rmse_vs_plain_by_slab": per_slab,
+            # per slab: rebin, split, Toeplitz GEMM, then the backprojection's kernels
+            "gpu_launches": (3 + fast_launches_per_bp(desc)) * nslabs * args.steps,
             "kernels": desc, "clocks": clocks.summary()}
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
 
 
-def run_batch(args, dev, world, rank, barrier):
+def run_batch(args, dev, world, rank, barrier, emit=True):
     """Twelve uneven scans (rotations 2..30, rows 16/32/64, three pitches, 256^2 or
     512^2 x 32..400 slices, Poisson noise at I0 = 2e5) through one BatchRecon:
     per-scan rebin + tensor-core filter, one persistent backprojection launch."""
@@ -604,11 +663,12 @@ def run_batch(args, dev, world, rank, barrier):
             "solo_fast_sum_ms": solo_ms, "batch_speedup_vs_solo": solo_ms / ms,
             "max_hu_rmse_vs_plain_solo": max(p["hu_rmse_vs_plain_solo"] for p in per_scan),
             "per_scan": per_scan, "kernels": desc, "clocks": clocks.summary()}
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
 
 
-def run_learned(args, dev, world, rank, barrier):
+def run_learned(args, dev, world, rank, barrier, emit=True):
     """Half-view (492 views/rot) plain reconstruction corrected by the 2.5D CNN,
     trained on pairs the plain method makes from seeded noisy phantoms, against
     the full-view (984 views/rot) plain reconstruction: HU RMSE on held-out
@@ -702,6 +762,7 @@ def run_learned(args, dev, world, rank, barrier):
     hu_learned, hu_half = hu["fast"]
     net.check()
     rf.close()
+    half_desc = rh["fast"].describe()
     for r in rh.values():
         r.close()
     # network FLOPs per slice: 2 * pixels * sum(9 * cin * cout) (padded channels counted)
@@ -736,11 +797,13 @@ def run_learned(args, dev, world, rank, barrier):
             "e2e": {"value": upd_half * world / s_learned / 1e9, "unit": "GUPS", "s_per_volume": s_learned,
                     "h2d_bytes_per_step": half.projection_bytes(), "d2h_bytes_per_step": half.volume_bytes(),
                     "entry": "HelicalRecon.run (fast form) + Corrector.apply_volume, pinned host fan in, volume out"},
-            # per learned step: rebin, split, Toeplitz GEMM, backprojection; then per 32-slice chunk the
-            # input packing and 8 conv layers
-            "gpu_launches": (4 + 9 * ((half.ZN + 31) // 32)) * args.steps, "clocks": clocks.summary()}
-    if rank == 0:
+            # per learned step: rebin, split, Toeplitz GEMM, the backprojection's kernels; then per 32-slice
+            # chunk the input packing and 8 conv layers
+            "gpu_launches": (3 + fast_launches_per_bp(half_desc) + 9 * ((half.ZN + 31) // 32)) * args.steps,
+            "clocks": clocks.summary()}
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -865,11 +928,44 @@ def main():
         gups_p, spv_p, detail_p = cpu_baseline(scan, budget_s=10.0, kind="port")
         line["cpu_port"] = {"value": gups_p, "unit": "GUPS", "cores": detail_p["cores"], "kind": "port",
                             "sample": detail_p["sample"], "s_per_volume": spv_p}
+    if args.config == "full" and world == 1 and not args.no_extra:
+        line.update(run_extras(args, dev, world, rank, barrier))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_extras(args, dev, world, rank, barrier):
+    """The other workloads, each run after the main one in the same process and
+    attached to its line: the 200-rotation big patient (slab pipeline), the
+    12-scan uneven batch and the learned half-view correction. Each keeps its
+    own value, e2e, error figure, launches and clocks."""
+    import torch
+
+    from analyticalreconbigpatient_b200 import geometry as G
+
+    sub = argparse.Namespace(**vars(args))
+    sub.steps = max(1, args.extra_steps)
+    sub.warmup = min(args.warmup, 3)
+    sub.e2e_steps = min(args.e2e_steps, 3)
+    out = {}
+    for name, fn in (("bigpatient", lambda: run_bigpatient(sub, G.config("bigpatient"), dev, world, rank, barrier,
+                                                            emit=False)),
+                     ("batch", lambda: run_batch(sub, dev, world, rank, barrier, emit=False)),
+                     ("learned", lambda: run_learned(sub, dev, world, rank, barrier, emit=False))):
+        t = time.perf_counter()
+        try:
+            res = fn()
+            res = {k: v for k, v in res.items() if k not in ("metric", "unit", "higher_is_better", "vs_baseline")}
+        except Exception as e:  # a failing sub-workload is reported, the main line stands
+            res = {"error": f"{type(e).__name__}: {e}"}
+        res["wall_s"] = time.perf_counter() - t
+        out[name] = res
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return out
 
 
 if __name__ == "__main__":

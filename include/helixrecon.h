@@ -279,11 +279,51 @@ void hr_recon_plan_destroy(hr_recon_plan* plan);
 typedef struct hr_slab_plan hr_slab_plan;
 int hr_slab_plan_create(hr_slab_plan** plan, const hr_recon_desc* desc, int slab_slices);
 /* fan [ViewN][YL][ZL], vol [YN][XN][ZN]; each on the host (pinned for overlap)
- * or the device as the flags say. Synchronous. */
+ * or the device as the flags say. Synchronous. Consecutive slabs' fan windows
+ * overlap; the shared views are copied on the device from the previous
+ * window, so each fan view crosses the host link once. */
 int hr_slab_execute(hr_slab_plan* plan, float* vol, const float* fan, int vol_on_host, int fan_on_host);
 int hr_slab_describe(const hr_slab_plan* plan, char* buf, int len);
 size_t hr_slab_device_bytes(const hr_slab_plan* plan);
 void hr_slab_plan_destroy(hr_slab_plan* plan);
+
+/* One scan on several GPUs: z slabs split between parts (one plan per GPU,
+ * part p of nparts), each part rebinning, filtering and backprojecting only
+ * its own slabs from its own fan windows and writing only their slices of the
+ * volume. No data cross between parts: windows of neighbouring parts overlap
+ * and the overlap is recomputed, which is cheaper than exchanging it. This
+ * replaces the reference's only way to split a long scan, the sequential
+ * segment loop (src/analyticalRecon.m:20-25), whose segments each need a
+ * volume-sized sum. */
+#define HR_SLAB_BLOCKS 0      /* part p takes a contiguous block of slabs (its fan views are one range) */
+#define HR_SLAB_ROUND_ROBIN 1 /* part p takes slabs p, p + nparts, ... */
+typedef struct hr_slab_window {
+  int slab;          /* slab index k: slices [k S, k S + n_slices) */
+  int first_slice, n_slices;
+  int bp_view0;      /* first backprojected view (cropped, rebinned numbering) */
+  int bp_views;      /* backprojection window length (the same for every slab) */
+  int fan_view0;     /* first fan view of the slab's window (view0 + bp_view0 - margin) */
+  int fan_views;     /* fan window length: bp_views + 2 margin (view0 of the desc) */
+  int shared_views;  /* leading fan views shared with the part's previous slab (0 for its first) */
+} hr_slab_window;
+/* The slab windows of part `part` of `nparts` (host arithmetic only, needs no
+ * GPU): *n = the part's slab count; out (cap entries, or NULL to query *n).
+ * The same arithmetic as hr_slab_plan_create_part. */
+int hr_slab_windows(const hr_recon_desc* desc, int slab_slices, int part, int nparts, int assign,
+                    hr_slab_window* out, int cap, int* n);
+/* Plan for part `part` of `nparts` (assign: HR_SLAB_BLOCKS or
+ * HR_SLAB_ROUND_ROBIN; nparts <= number of slabs). hr_slab_plan_create is
+ * part 0 of 1. */
+int hr_slab_plan_create_part(hr_slab_plan** plan, const hr_recon_desc* desc, int slab_slices, int part, int nparts,
+                             int assign);
+/* As hr_slab_execute, with fan holding views [fan_view0, ...) of the scan
+ * only (at least the range hr_slab_fan_range reports): a part needs only its
+ * own views in memory. */
+int hr_slab_execute_range(hr_slab_plan* plan, float* vol, const float* fan, int fan_view0, int vol_on_host,
+                          int fan_on_host);
+/* Fan views the plan reads, [first_view, first_view + nviews), and the bytes
+ * one execution copies from the caller's fan (overlaps counted once). */
+int hr_slab_fan_range(const hr_slab_plan* plan, int* first_view, int* nviews, size_t* bytes_per_execute);
 
 /* ---- several scans of uneven size in one persistent launch --------------- */
 /* n (1..16) independent scans, each described as for hr_recon_plan_create

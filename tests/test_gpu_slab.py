@@ -47,3 +47,43 @@ def test_slabs_match_whole_scan_fast_chain(cuda, slab, dz):
     assert np.array_equal(vol_h.numpy(), got)
     rec.close()
 
+
+
+@pytest.mark.parametrize("assign", [_lib.HR_SLAB_BLOCKS, _lib.HR_SLAB_ROUND_ROBIN])
+def test_parts_of_one_scan_compose_the_whole(cuda, assign):
+    """The slabs of one scan split between plans (part p of 3, as ranks on three
+    GPUs would hold them; here run one after the other on one GPU): every plan
+    writes only its own slices, each from only its own fan views, and together
+    they give the single plan's volume bit for bit (same kernel variant)."""
+    import os
+
+    from analyticalreconbigpatient_b200.pipeline import slab_windows
+
+    sc = G.Scan(ZL=16, pitch=0.9375, rotations=6, XN=64, YN=64, ZN=1, dx=4.0, dy=4.0, dz=1.5)
+    sc = G.Scan(**{**sc.__dict__, "ZN": sc.fully_sampled_slices() + 2})
+    zlo, zhi = sc.h * sc.BetaS / (2 * np.pi), -sc.h * sc.BetaS / (2 * np.pi)
+    fan = project(sc, P.random_ellipsoids(12, 20, (zlo, zhi), body=(110.0, 90.0), semi_axes=(5, 40)))
+    os.environ["HELIXRECON_BP_VARIANT"] = "11"
+    try:
+        whole_plan = SlabRecon(sc, slab_slices=8)
+        ref = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
+        whole_plan.run(fan, ref)
+        first, count, nbytes = whole_plan.fan_range()
+        whole_plan.close()
+        per_view = sc.YL * sc.ZL * 4
+        # each fan view crosses from the caller's buffer once (overlaps are copied on the device)
+        assert nbytes == count * per_view and first + count <= sc.views
+        got = torch.full_like(ref, float("nan"))
+        for part in range(3):
+            rec = SlabRecon(sc, slab_slices=8, part=part, nparts=3, assign=assign)
+            f0, n, _ = rec.fan_range()
+            only_mine = fan[f0: f0 + n].clone()  # the part's views and nothing else
+            rec.run(only_mine, got, fan_view0=f0)
+            assert f"part {part} of 3" in rec.describe()
+            rec.close()
+    finally:
+        del os.environ["HELIXRECON_BP_VARIANT"]
+    wins = [w for p in range(3) for w in slab_windows(sc, 8, p, 3, assign)]
+    assert sorted(w["slab"] for w in wins) == list(range(-(-sc.ZN // 8)))
+    assert torch.isfinite(got).all()
+    assert torch.equal(got, ref)
