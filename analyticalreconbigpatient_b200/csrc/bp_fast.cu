@@ -521,6 +521,111 @@ __global__ void __launch_bounds__(kBx* kBy) bp_tex_kernel(float* __restrict__ vo
   tex_column<NZ>(vol, X, T, P, xi, yi, b_first + blockIdx.z);
 }
 
+// ---- segmented texture variants ----
+// A z block's union window, cut into segments over which the slices holding
+// the view are a fixed range [MA, MB] (the table's view masks, built on the
+// host): slices entering at the start of the window and leaving at its end
+// cost nothing outside their own windows. Per slice the views are visited in
+// the same order with the same operations as tex_column (a slice without the
+// view added exactly 0 there), so both give the same bits.
+struct SegCtx {
+  const float2* trig;
+  const float4* btab;  // the block's first table row, two slices per float4
+  const unsigned long long* texs;
+  float x, y, utop, vtop, zlch;
+  int blk0, lsh, lmask;
+};
+
+template <int NZ, int MA, int MB>
+__device__ __forceinline__ void tex_range(float (&res)[NZ], const SegCtx& c, const FastParams& P, int q0, int q1) {
+#pragma unroll 1
+  for (int q = q0; q < q1; ++q) {
+    const int p = c.blk0 + q;
+    const float2 cs = __ldg(c.trig + p);
+    const float UU = -c.x * cs.x - c.y * cs.y;
+    const float Yr = -c.x * cs.y + c.y * cs.x;
+    const float u1 = fmaf(Yr, P.invdYL, P.YLC0);
+    if (!(u1 >= 0.0f && u1 < c.utop)) continue;  // floor(u1) in [0, YL-2]
+    const float t1sq = P.SO2 - Yr * Yr;
+    const float temp1 = t1sq * rsqrtf(t1sq);
+    const float A = temp1 + UU, B = temp1 - UU;
+    const float K = P.SOSDdZL * rcp_approx(temp1 * A);
+    const float E = ex2_approx(P.k1 * lg2_approx(B * rcp_approx(A)));
+    const cudaTextureObject_t tx = __ldg(c.texs + (p >> c.lsh));
+    const int layer = p & c.lmask;
+    const float xt = u1 + 0.5f;
+    const float4* e = c.btab + (size_t)q * (NZ / 2);
+    float tap[NZ], qv[NZ];
+#pragma unroll
+    for (int cc = MA / 2; cc <= MB / 2; ++cc) {
+      const float4 t = __ldg(e + cc);  // {t2, 2^Q} of slices 2cc and 2cc+1
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int m = 2 * cc + i;
+        if (m < MA || m > MB) continue;
+        qv[m] = i ? t.w : t.y;
+        const float vh = fmaf(i ? t.z : t.x, K, c.zlch);  // row position + 1/2
+        const bool ok = vh >= 0.5f && vh < c.vtop;
+        tap[m] = ok ? tex2DLayered<float>(tx, xt, vh, layer) : 0.0f;
+      }
+    }
+#pragma unroll
+    for (int m = MA; m <= MB; ++m) res[m] = fmaf(rcp_approx(fmaf(qv[m], E, 1.0f)), tap[m], res[m]);
+  }
+}
+
+// Runs segment sg = {q0, q1, ma, mb} with the code specialised for its range.
+template <int NZ, int MA, int MB>
+__device__ __forceinline__ void tex_dispatch(float (&res)[NZ], const SegCtx& c, const FastParams& P, int4 sg) {
+  if (sg.z == MA && sg.w == MB) {
+    tex_range<NZ, MA, MB>(res, c, P, sg.x, sg.y);
+    return;
+  }
+  if constexpr (MB + 1 < NZ)
+    tex_dispatch<NZ, MA, MB + 1>(res, c, P, sg);
+  else if constexpr (MA + 1 < NZ)
+    tex_dispatch<NZ, MA + 1, MA + 1>(res, c, P, sg);
+}
+
+template <int NZ>
+__global__ void __launch_bounds__(kBx* kBy) bp_tex_seg_kernel(float* __restrict__ vol, const TexRef X, const ZTabs T,
+                                                             const int4* __restrict__ segs, const FastParams P,
+                                                             int b_first) {
+  static_assert(NZ % 2 == 0, "table entries are read two slices at a time");
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  if (xi >= P.XN || yi >= P.YN) return;
+  const int b = b_first + blockIdx.z;
+  const int z0 = b * NZ;
+  SegCtx c;
+  c.trig = T.trig;
+  c.btab = reinterpret_cast<const float4*>(T.ztab + (size_t)T.zoff[b] * NZ);
+  c.texs = X.texs;
+  c.x = ((float)xi - P.XNC) * P.dx;
+  c.y = ((float)yi - P.YNC) * P.dy;
+  c.utop = (float)(P.YL - 1);
+  c.vtop = (float)P.ZL - 0.5f;
+  c.zlch = P.ZLC0 + 0.5f;
+  c.blk0 = T.zblock[b].x;
+  c.lsh = X.lsh;
+  c.lmask = (1 << X.lsh) - 1;
+  float res[NZ];
+#pragma unroll
+  for (int m = 0; m < NZ; ++m) res[m] = 0.0f;
+  const int4* sb = segs + (size_t)b * (hr::kSegPerNz * NZ);
+#pragma unroll 1
+  for (int sgi = 0; sgi < hr::kSegPerNz * NZ; ++sgi) {
+    const int4 sg = __ldg(sb + sgi);
+    if (sg.x >= sg.y) continue;  // unused entry (uniform over the CTA)
+    tex_dispatch<NZ, 0, 0>(res, c, P, sg);
+  }
+  const float outs = P.DeltaFai * __ldg(X.scale);
+  float* out = vol + ((size_t)yi * P.XN + xi) * P.ZN + z0;
+#pragma unroll
+  for (int m = 0; m < NZ; ++m)
+    if (z0 + m < P.ZN) out[m] = res[m] * outs;
+}
+
 // The persistent multi-scan launch with texture taps: the work items and
 // their claiming as in bp_fast_batch_kernel; each scan samples its own arrays
 // with 8 or 4 slices per thread (NZF = 0: the scan's own choice) or 4 for all
@@ -643,6 +748,35 @@ static int build_host(BpFastHostSet* t, int NZ, const BpFastGeom& g, const doubl
       t->mask[row] = mk;
     }
   }
+  // view segments of each block for the segmented variants: runs of views
+  // with the same active range [lowest, highest slice of the mask]; views no
+  // slice needs are dropped; a block whose runs exceed the capacity keeps one
+  // segment over its whole window (slices without a view sample nothing)
+  const int cap = kSegPerNz * NZ;
+  t->seg.assign((size_t)nblocks * cap, make_int4(0, 0, 0, 0));
+  std::vector<int4> sv;
+  for (int b = 0; b < nblocks; ++b) {
+    sv.clear();
+    const size_t r0 = (size_t)t->zb[2 * nblocks + b];
+    for (int q = 0; q < t->zb[2 * b + 1]; ++q) {
+      const uint32_t mk = t->mask[r0 + q];
+      if (mk == 0u) continue;
+      const int ma = __builtin_ctz(mk), mb = 31 - __builtin_clz(mk);
+      if (!sv.empty() && sv.back().y == q && sv.back().z == ma && sv.back().w == mb)
+        sv.back().y = q + 1;
+      else
+        sv.push_back(make_int4(q, q + 1, ma, mb));
+    }
+    if ((int)sv.size() > cap) {
+      int4 all = make_int4(sv.front().x, sv.back().y, NZ, -1);
+      for (const int4& g : sv) {
+        all.z = std::min(all.z, g.z);
+        all.w = std::max(all.w, g.w);
+      }
+      sv.assign(1, all);
+    }
+    std::copy(sv.begin(), sv.end(), t->seg.begin() + (size_t)b * cap);
+  }
   return HR_OK;
 }
 
@@ -666,7 +800,9 @@ int bp_fast_reserve(BpFast* f, const size_t rows[kFastTableSets], const int nblo
     HR_CUDA_TRY(cudaMalloc(&t.d_tab, sizeof(float2) * t.cap_rows * t.nz));
     HR_CUDA_TRY(cudaMalloc(&t.d_mask, sizeof(uint32_t) * t.cap_rows));
     HR_CUDA_TRY(cudaMalloc(&t.d_zblock, sizeof(int) * 3 * (size_t)t.nblocks));
-    t.bytes = (sizeof(float2) * t.nz + sizeof(uint32_t)) * t.cap_rows + sizeof(int) * 3 * (size_t)t.nblocks;
+    HR_CUDA_TRY(cudaMalloc(&t.d_seg, sizeof(int4) * kSegPerNz * t.nz * (size_t)t.nblocks));
+    t.bytes = (sizeof(float2) * t.nz + sizeof(uint32_t)) * t.cap_rows + sizeof(int) * 3 * (size_t)t.nblocks +
+              sizeof(int4) * kSegPerNz * t.nz * (size_t)t.nblocks;
     f->bytes += t.bytes;
   }
   f->cap_views = PN;
@@ -685,6 +821,7 @@ int bp_fast_upload(BpFast* f, const BpFastHost& h, cudaStream_t s) {
     HR_CUDA_TRY(cudaMemcpyAsync(t.d_mask, ht.mask.data(), sizeof(uint32_t) * ht.mask.size(), cudaMemcpyHostToDevice,
                                 s));
     HR_CUDA_TRY(cudaMemcpyAsync(t.d_zblock, ht.zb.data(), sizeof(int) * ht.zb.size(), cudaMemcpyHostToDevice, s));
+    HR_CUDA_TRY(cudaMemcpyAsync(t.d_seg, ht.seg.data(), sizeof(int4) * ht.seg.size(), cudaMemcpyHostToDevice, s));
   }
   HR_REQUIRE(h.trig.size() <= (size_t)f->cap_views, "fast backprojection: more views than reserved");
   HR_CUDA_TRY(cudaMemcpyAsync(f->d_trig, h.trig.data(), sizeof(float2) * h.trig.size(), cudaMemcpyHostToDevice, s));
@@ -807,6 +944,7 @@ void bp_fast_destroy(BpFast* f) {
     cudaFree(f->t[i].d_tab);
     cudaFree(f->t[i].d_mask);
     cudaFree(f->t[i].d_zblock);
+    cudaFree(f->t[i].d_seg);
   }
   cudaFree(f->d_trig);
   *f = BpFast{};
@@ -846,6 +984,13 @@ static void launch_tex(const BpFastTables& t, const BpFast& f, const FastParams&
   bp_tex_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), P, b_first);
 }
 
+template <int NZ>
+static void launch_tex_seg(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol, int b_first,
+                           int b_count, cudaStream_t s) {
+  dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
+  bp_tex_seg_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), t.d_seg, P, b_first);
+}
+
 // Launches variant v over z blocks [b_first, b_first + b_count) (count < 0: all).
 static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, const uint32_t* fpb, int b_first,
                        int b_count, cudaStream_t s) {
@@ -858,10 +1003,17 @@ static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, 
   if (fv.tex) {
     HR_REQUIRE(f.tex.kind == fv.tex && f.tex.views >= g.PN, "fast backprojection: the textures of variant %d are "
                "not prepared", v);
-    switch (kFastNz[fv.table]) {
-      case 16: launch_tex<16>(t, f, P, vol, b_first, b_count, s); break;
-      case 8: launch_tex<8>(t, f, P, vol, b_first, b_count, s); break;
-      default: launch_tex<4>(t, f, P, vol, b_first, b_count, s); break;
+    if (fv.seg) {
+      if (kFastNz[fv.table] == 8)
+        launch_tex_seg<8>(t, f, P, vol, b_first, b_count, s);
+      else
+        launch_tex_seg<4>(t, f, P, vol, b_first, b_count, s);
+    } else {
+      switch (kFastNz[fv.table]) {
+        case 16: launch_tex<16>(t, f, P, vol, b_first, b_count, s); break;
+        case 8: launch_tex<8>(t, f, P, vol, b_first, b_count, s); break;
+        default: launch_tex<4>(t, f, P, vol, b_first, b_count, s); break;
+      }
     }
     HR_CUDA_TRY(cudaGetLastError());
     return HR_OK;
@@ -1098,7 +1250,8 @@ int bp_fast_describe(const BpFast& f, char* buf, int len) {
   if (!buf || len <= 0) return HR_OK;
   const FastVariant& fv = kFastVariants[f.variant];
   int n = snprintf(buf, (size_t)len, "slices_per_thread=%d gathers=%s tile=%dx%d %s", kFastNz[fv.table],
-                   fv.tex == kTexHalf ? "texture-fp16" : fv.tex == kTexFloat ? "texture-fp32"
+                   fv.tex == kTexHalf ? (fv.seg ? "texture-fp16-segmented" : "texture-fp16")
+                   : fv.tex == kTexFloat ? "texture-fp32"
                    : fv.chunk < 0 ? "paired-f32x2" : fv.chunk == 0 ? "per-slice" : fv.chunk == 4 ? "chunk4" : "chunk8",
                    kBx, kBy, f.tuned == 2 ? "(pinned by HELIXRECON_BP_VARIANT)"
                    : f.tuned ? "(autotuned; ms/slice:" : "(default)");

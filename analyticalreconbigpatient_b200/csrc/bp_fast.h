@@ -29,13 +29,19 @@ constexpr int kFastNz[kFastTableSets] = {16, 8, 4};
 // the texture units' bilinear filtering of a layered copy of the filtered data
 // (kTexHalf: FP16 scaled by a power of two; kTexFloat: FP32).
 constexpr int kTexHalf = 1, kTexFloat = 2;
+// seg != 0 (texture variants with 8 or 4 slices per thread): the view loop of
+// a z block runs in segments over which the set of slices whose window holds
+// the view is a fixed range [ma, mb], with code specialised for that range, so
+// slices without the view cost nothing (thick slices: a block's union window
+// is much longer than one slice's).
 struct FastVariant {
-  int table, chunk, tex;
+  int table, chunk, tex, seg;
 };
 constexpr FastVariant kFastVariants[] = {{0, 0}, {0, 4}, {0, 8}, {1, 0}, {1, 4}, {1, 8},
                                          {0, -1}, {1, -1}, {2, 0}, {2, -1}, {2, 4},
                                          {1, 0, kTexHalf}, {0, 0, kTexHalf}, {2, 0, kTexHalf},
-                                         {1, 0, kTexFloat}, {0, 0, kTexFloat}};
+                                         {1, 0, kTexFloat}, {0, 0, kTexFloat},
+                                         {1, 0, kTexHalf, 1}, {2, 0, kTexHalf, 1}};
 constexpr int kFastVariants_n = sizeof(kFastVariants) / sizeof(kFastVariants[0]);
 constexpr int kFastDefaultVariant = 0;
 
@@ -43,12 +49,17 @@ constexpr int kFastDefaultVariant = 0;
 // kernel parameter block).
 constexpr int kBatchMaxScans = 16;
 
+// View segments per z block of the segmented variants: {q0, q1, ma, mb}, views
+// [q0, q1) of the block's window with active slices [ma, mb] (q0 == q1: unused).
+constexpr int kSegPerNz = 2;  // at most 2 NZ segments per block (NZ - 1 entering, 1 full, NZ - 1 leaving)
+
 struct BpFastTables {
   int nz = 0, nblocks = 0;
   size_t cap_rows = 0;         // reserved table rows (views summed over blocks)
   float2* d_tab = nullptr;     // per z block and view of its window: NZ x {t2, 2^Q}
   uint32_t* d_mask = nullptr;  // per z block and view: slices whose [s1, s2] holds the view
   int* d_zblock = nullptr;     // [nblocks] {first view, count}, then [nblocks] table offsets
+  int4* d_seg = nullptr;       // [nblocks][kSegPerNz NZ] view segments
   size_t bytes = 0;
 };
 
@@ -58,6 +69,7 @@ struct BpFastHostSet {
   std::vector<float2> tab;
   std::vector<uint32_t> mask;
   std::vector<int> zb;
+  std::vector<int4> seg;
 };
 struct BpFastHost;
 

@@ -199,8 +199,10 @@ int hr_bp_describe(const hr_bp_plan* plan, char* buf, int len);
  * slice pairs; 8-10 four slices per thread, per slice / pairs / batched;
  * 11-13 eight / sixteen / four slices per thread sampling an FP16 layered
  * texture copy of the data with the texture units' bilinear filtering, 14-15
- * eight / sixteen with an FP32 copy; the texture variants allocate the copy,
- * 2 or 4 bytes per sample, and fill it on every execution).
+ * eight / sixteen with an FP32 copy, 16-17 eight / four slices per thread
+ * from the FP16 copy with the view loop cut into segments of a fixed set of
+ * slices holding the view (thick slices); the texture variants allocate the
+ * copy, 2 or 4 bytes per sample, and fill it on every execution).
  * For tests and manual tuning. */
 int hr_bp_select(hr_bp_plan* plan, int variant);
 

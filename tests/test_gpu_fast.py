@@ -124,7 +124,7 @@ def test_every_fast_variant_gives_the_same_volume(cuda, pixel):
     fast.pack(pairs, filt)
     lib = _lib.load()
     vols = []
-    nvar = 16
+    nvar = 18
     for v in range(nvar):
         _lib.check(lib.hr_bp_select(fast._bp, v))
         vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
@@ -145,6 +145,8 @@ def test_every_fast_variant_gives_the_same_volume(cuda, pixel):
         assert rel_l2(vols[v], vols[0]) < 1e-2, (v, rel_l2(vols[v], vols[0]))
     assert np.array_equal(vols[11], vols[12]) and np.array_equal(vols[11], vols[13])
     assert np.array_equal(vols[14], vols[15])
+    # segmented view loops (16: 8 slices per thread, 17: 4): same operations per slice and view
+    assert np.array_equal(vols[16], vols[11]) and np.array_equal(vols[17], vols[13])
     assert np.isfinite(vols[0]).all()
 
 
