@@ -21,6 +21,18 @@
 // again and stored. The input may be in the reference's row
 // layout [v][ZL][YL] or in the rebinning's layout [v][YL][ZL]; for the latter
 // the 4 rows of a tile are 16 contiguous bytes per channel.
+//
+// N = 2048 (YL in (512, 1024], the scanners' 888 channels) runs a register-
+// resident kernel instead: one warp per pair of rows, 64 points per lane
+// (N = 64 x 32). Forward: each lane j transforms x[j + 32 m] over m with a
+// 64-point DFT (8 x 8, in registers), multiplies by W_2048^(j c), and the
+// warp exchanges through shared memory so that lane t holds columns c = t,
+// t+32 for all j; a 32-point DFT over j (4 x 8) gives frequencies c + 64 q,
+// which are multiplied by H. The inverse runs the same steps backwards: a
+// 32-point inverse DFT over q, the conjugate twiddle, an exchange back, and
+// a 64-point inverse DFT per lane gives y[j + 32 n] in registers, stored
+// straight to the output rows. Two shared-memory exchanges per pair of rows,
+// no block-wide barrier after set-up.
 #include <cmath>
 #include <vector>
 
@@ -31,6 +43,8 @@ struct hr_filter_plan {
   float PLC, ZLC, dYL, dZL, SO;
   float* d_H;    // real spectrum of the wrapped kernel, divided by N
   float2* d_tw;  // exp(-2 pi i t / N), t in [0, N)
+  float* d_wt;   // N = 2048: preweight of every (row k, channel j), [ZL][YL]
+  float2* d_tw2; // N = 2048: W_2048^(j c) as [c][j], c in [0, 64), j in [0, 32)
 };
 
 namespace {
@@ -188,6 +202,264 @@ __global__ void __launch_bounds__(kThreads) filter_fft_kernel(float* __restrict_
   }
 }
 
+// ---------------------------------------------------------------------------
+// N = 2048: register-resident transforms, one warp per row pair.
+// ---------------------------------------------------------------------------
+namespace fft2k {
+
+constexpr int kN = 2048;
+constexpr int kWarps = 4;      // row pairs in flight per CTA
+constexpr int kStride = 66;    // exchange row stride in float2 (64 + 2: 16-byte lanes hit distinct banks)
+
+// W_64^x (forward), x in [0, 64); W_32^x = W_64^(2x).
+__constant__ float2 c_w64[64];
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// a * w (INV: a * conj(w))
+template <bool INV>
+__device__ __forceinline__ float2 cmulw(float2 a, float2 w) {
+  return INV ? make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y)
+             : make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+// a * (-i) forward, a * (+i) inverse
+template <bool INV>
+__device__ __forceinline__ float2 rot(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+// a * W_8 (forward (1 - i)/sqrt 2, inverse (1 + i)/sqrt 2)
+template <bool INV>
+__device__ __forceinline__ float2 w8(float2 a) {
+  const float r = 0.70710678118654752f;
+  return INV ? make_float2((a.x - a.y) * r, (a.x + a.y) * r) : make_float2((a.x + a.y) * r, (a.y - a.x) * r);
+}
+
+// 4-point DFT of v[O], v[O+S], v[O+2S], v[O+3S], in place, natural order.
+template <bool INV, int O, int S, int L>
+__device__ __forceinline__ void dft4(float2 (&v)[L]) {
+  const float2 t0 = cadd(v[O], v[O + 2 * S]), t1 = csub(v[O], v[O + 2 * S]);
+  const float2 t2 = cadd(v[O + S], v[O + 3 * S]), t3 = rot<INV>(csub(v[O + S], v[O + 3 * S]));
+  v[O] = cadd(t0, t2);
+  v[O + 2 * S] = csub(t0, t2);
+  v[O + S] = cadd(t1, t3);
+  v[O + 3 * S] = csub(t1, t3);
+}
+
+// 8-point DFT of v[O + S i], i in [0, 8), in place, natural order (even/odd split).
+template <bool INV, int O, int S, int L>
+__device__ __forceinline__ void dft8(float2 (&v)[L]) {
+  dft4<INV, O, 2 * S>(v);      // E[k] at v[O + 2S k]
+  dft4<INV, O + S, 2 * S>(v);  // O[k] at v[O + S + 2S k]
+  const float2 e0 = v[O], e1 = v[O + 2 * S], e2 = v[O + 4 * S], e3 = v[O + 6 * S];
+  const float2 o0 = v[O + S], o1 = w8<INV>(v[O + 3 * S]), o2 = rot<INV>(v[O + 5 * S]);
+  const float2 o3 = rot<INV>(w8<INV>(v[O + 7 * S]));
+  v[O] = cadd(e0, o0);
+  v[O + 4 * S] = csub(e0, o0);
+  v[O + S] = cadd(e1, o1);
+  v[O + 5 * S] = csub(e1, o1);
+  v[O + 2 * S] = cadd(e2, o2);
+  v[O + 6 * S] = csub(e2, o2);
+  v[O + 3 * S] = cadd(e3, o3);
+  v[O + 7 * S] = csub(e3, o3);
+}
+
+template <bool INV, int M2>
+__device__ __forceinline__ void dft64_cols(float2 (&v)[64]) {
+  dft8<INV, M2, 8>(v);
+  if constexpr (M2 + 1 < 8) dft64_cols<INV, M2 + 1>(v);
+}
+template <bool INV, int K1>
+__device__ __forceinline__ void dft64_rows(float2 (&v)[64]) {
+  dft8<INV, 8 * K1, 1>(v);
+  if constexpr (K1 + 1 < 8) dft64_rows<INV, K1 + 1>(v);
+}
+// 64-point DFT of v (natural order in); position 8 k1 + k2 ends up holding
+// frequency k1 + 8 k2.
+template <bool INV>
+__device__ __forceinline__ void dft64(float2 (&v)[64]) {
+  dft64_cols<INV, 0>(v);  // over m1 for each m2: position m2 + 8 k1
+#pragma unroll
+  for (int m2 = 1; m2 < 8; ++m2)
+#pragma unroll
+    for (int k1 = 1; k1 < 8; ++k1) v[m2 + 8 * k1] = cmulw<INV>(v[m2 + 8 * k1], c_w64[m2 * k1]);
+  dft64_rows<INV, 0>(v);  // over m2 for each k1: position 8 k1 + k2
+}
+__device__ __forceinline__ int dft64_freq(int p) { return (p >> 3) + 8 * (p & 7); }
+
+template <int M2>
+__device__ __forceinline__ void dft32f_cols(float2 (&v)[32]) {
+  dft8<false, M2, 4>(v);
+  if constexpr (M2 + 1 < 4) dft32f_cols<M2 + 1>(v);
+}
+template <int Q1>
+__device__ __forceinline__ void dft32f_rows(float2 (&v)[32]) {
+  dft4<false, 4 * Q1, 1>(v);
+  if constexpr (Q1 + 1 < 8) dft32f_rows<Q1 + 1>(v);
+}
+// Forward 32-point DFT (natural order in); position 4 q1 + q2 ends up holding
+// frequency q1 + 8 q2.
+__device__ __forceinline__ void dft32_fwd(float2 (&v)[32]) {
+  dft32f_cols<0>(v);  // over m1 for each m2 (j = m2 + 4 m1): position m2 + 4 q1
+#pragma unroll
+  for (int m2 = 1; m2 < 4; ++m2)
+#pragma unroll
+    for (int q1 = 1; q1 < 8; ++q1) v[m2 + 4 * q1] = cmulw<false>(v[m2 + 4 * q1], c_w64[2 * m2 * q1]);
+  dft32f_rows<0>(v);  // over m2 for each q1
+}
+template <int Q1>
+__device__ __forceinline__ void dft32i_rows(float2 (&v)[32]) {
+  dft4<true, 4 * Q1, 1>(v);
+  if constexpr (Q1 + 1 < 8) dft32i_rows<Q1 + 1>(v);
+}
+template <int R1>
+__device__ __forceinline__ void dft32i_cols(float2 (&v)[32]) {
+  dft8<true, R1, 4>(v);
+  if constexpr (R1 + 1 < 4) dft32i_cols<R1 + 1>(v);
+}
+// Inverse 32-point DFT whose input is in dft32_fwd's output order; the
+// output is in natural order.
+__device__ __forceinline__ void dft32_inv(float2 (&v)[32]) {
+  dft32i_rows<0>(v);  // over q2 for each q1: position 4 q1 + r1
+#pragma unroll
+  for (int r1 = 1; r1 < 4; ++r1)
+#pragma unroll
+    for (int q1 = 1; q1 < 8; ++q1) v[4 * q1 + r1] = cmulw<true>(v[4 * q1 + r1], c_w64[2 * r1 * q1]);
+  dft32i_cols<0>(v);  // over q1 for each r1: position r1 + 4 r2 = n
+}
+__device__ __forceinline__ int dft32_freq(int p) { return (p >> 2) + 8 * (p & 3); }
+
+// Preweight table [ZL][YL] with the reference's float expression
+// (src/filtering.cu:187-207).
+__global__ void preweight_table_kernel(float* __restrict__ wt, int YL, int ZL, float PLC, float ZLC, float dYL,
+                                       float dZL, float SO) {
+  const float SO2 = SO * SO;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < YL * ZL; e += gridDim.x * blockDim.x) {
+    const int k = e / YL, j = e - k * YL;
+    const float b = ((float)k - ZLC) * dZL;
+    const float t = ((float)j - PLC) * dYL;
+    wt[e] = SO2 / sqrtf(SO2 * (SO2 + b * b) - b * t * b * t);
+  }
+}
+
+template <int IN_LAYOUT>
+__global__ void __launch_bounds__(32 * kWarps, 3) filter2048_kernel(float* __restrict__ out, const float* __restrict__ in,
+                                                                const float* __restrict__ gH,
+                                                                const float2* __restrict__ gtw2,
+                                                                const float* __restrict__ wt, int YL, int ZL,
+                                                                long long rows, int view0) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tw2 = reinterpret_cast<float2*>(smem_raw);             // [64][32]
+  float* H = reinterpret_cast<float*>(tw2 + 64 * 32);            // [2048]
+  float2* xbuf = reinterpret_cast<float2*>(H + kN) + (threadIdx.x >> 5) * (32 * kStride);  // this warp's exchange
+  for (int t = threadIdx.x; t < 64 * 32; t += blockDim.x) tw2[t] = gtw2[t];
+  for (int t = threadIdx.x; t < kN; t += blockDim.x) H[t] = gH[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long pairs = (rows + 1) >> 1;
+  const long long warps = (long long)gridDim.x * kWarps;
+  for (long long pr = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5); pr < pairs; pr += warps) {
+    const long long ra = 2 * pr, rb = ra + 1;
+    const bool hasb = rb < rows;
+    const int ka = (int)(ra % ZL), kb = (int)(rb % ZL);
+    const long long va = ra / ZL, vb = rb / ZL;
+    // ---- load x[n] = wa[n] a[n] + i wb[n] b[n], n = lane + 32 m, and the first
+    // stage of the 64-point DFT (over m1, m = m2 + 8 m1) group by group --------
+    const float* pa = IN_LAYOUT == HR_LAYOUT_ROWS ? in + ((size_t)(view0 + va) * ZL + ka) * YL
+                                                  : in + (size_t)(view0 + va) * YL * ZL + ka;
+    const float* pb = IN_LAYOUT == HR_LAYOUT_ROWS ? in + ((size_t)(view0 + vb) * ZL + kb) * YL
+                                                  : in + (size_t)(view0 + vb) * YL * ZL + kb;
+    const size_t es = IN_LAYOUT == HR_LAYOUT_ROWS ? 1 : (size_t)ZL;  // element stride along a row
+    const float* wa = wt + (size_t)ka * YL;
+    const float* wb = wt + (size_t)kb * YL;
+    float2 v[64];
+#pragma unroll
+    for (int m2 = 0; m2 < 8; ++m2) {
+#pragma unroll
+      for (int m1 = 0; m1 < 8; ++m1) {
+        const int n = lane + 32 * (m2 + 8 * m1);
+        float a = 0.0f, b = 0.0f;
+        if (n < YL) {
+          a = __ldg(pa + n * es) * __ldg(wa + n);
+          if (hasb) b = __ldg(pb + n * es) * __ldg(wb + n);
+        }
+        v[m2 + 8 * m1] = make_float2(a, b);
+      }
+      asm volatile("" ::: "memory");  // keep each group's loads next to its use
+    }
+    __syncwarp();  // the previous pair's reads of xbuf are done
+#pragma unroll
+    for (int k1 = 0; k1 < 8; k1 += 2)
+#pragma unroll
+      for (int k2 = 0; k2 < 8; ++k2) {
+        const int c = k1 + 8 * k2;  // even
+        const float2 x0 = cmulw<false>(v[8 * k1 + k2], tw2[c * 32 + lane]);
+        const float2 x1 = cmulw<false>(v[8 * (k1 + 1) + k2], tw2[(c + 1) * 32 + lane]);
+        *reinterpret_cast<float4*>(xbuf + lane * kStride + c) = make_float4(x0.x, x0.y, x1.x, x1.y);
+      }
+    __syncwarp();
+    // lane t owns columns c = t and t + 32 (all j): it reads each, transforms
+    // it and writes it back in place (no other lane touches the column)
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) {
+      const int c = lane + 32 * half;
+      float2 y[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) y[j] = xbuf[j * kStride + c];
+      // ---- 32-point DFT over j, H, inverse 32-point DFT over q -------------
+      dft32_fwd(y);
+#pragma unroll
+      for (int p = 0; p < 32; ++p) {
+        const float h = H[c + 64 * dft32_freq(p)];
+        y[p] = make_float2(y[p].x * h, y[p].y * h);
+      }
+      dft32_inv(y);
+      // ---- twiddle conj(W_2048^(n c)), back into the column ------------------
+#pragma unroll
+      for (int n = 0; n < 32; ++n) xbuf[n * kStride + c] = cmulw<true>(y[n], tw2[c * 32 + n]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 64; c += 2) {
+      const float4 q = *reinterpret_cast<const float4*>(xbuf + lane * kStride + c);
+      v[c] = make_float2(q.x, q.y);
+      v[c + 1] = make_float2(q.z, q.w);
+    }
+    // ---- inverse 64-point DFTs over c: y[lane + 32 n] ------------------------
+    dft64<true>(v);
+    float* oa = out + (size_t)ra * YL;
+    float* ob = out + (size_t)rb * YL;
+#pragma unroll
+    for (int p = 0; p < 64; ++p) {
+      const int n = lane + 32 * dft64_freq(p);
+      if (n < YL) {
+        oa[n] = v[p].x;
+        if (hasb) ob[n] = v[p].y;
+      }
+    }
+  }
+}
+
+size_t smem_bytes() { return 64 * 32 * sizeof(float2) + kN * sizeof(float) + kWarps * 32 * kStride * sizeof(float2); }
+
+template <int IN_LAYOUT>
+int launch(const hr_filter_plan* p, float* out, const float* in, int view0, cudaStream_t s) {
+  auto kern = filter2048_kernel<IN_LAYOUT>;
+  const size_t smem = smem_bytes();
+  HR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long rows = (long long)p->ZL * p->ViewN;
+  const long long tiles = ((rows + 1) / 2 + kWarps - 1) / kWarps;
+  int per_sm = 0;
+  HR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kWarps, smem));
+  if (per_sm < 1) per_sm = 1;
+  const long long want = (long long)per_sm * hr::sm_count();
+  const int grid = (int)(tiles < want ? tiles : want);
+  kern<<<grid, 32 * kWarps, smem, s>>>(out, in, p->d_H, p->d_tw2, p->d_wt, p->YL, p->ZL, rows, view0);
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
+}  // namespace fft2k
+
 size_t smem_bytes(int log2N) {
   const size_t N = (size_t)1 << log2N;
   return 2 * kRowPairs * N * sizeof(float2) + N * sizeof(float2) + N * sizeof(float);
@@ -222,7 +494,7 @@ int launch_layout(const hr_filter_plan* p, float* out, const float* in, int view
     case 8: return launch_t<8, IN_LAYOUT>(p, out, in, view0, s);
     case 9: return launch_t<9, IN_LAYOUT>(p, out, in, view0, s);
     case 10: return launch_t<10, IN_LAYOUT>(p, out, in, view0, s);
-    case 11: return launch_t<11, IN_LAYOUT>(p, out, in, view0, s);
+    case 11: return fft2k::launch<IN_LAYOUT>(p, out, in, view0, s);
     case 12: return launch_t<12, IN_LAYOUT>(p, out, in, view0, s);
     default: return hr::fail(HR_ERR_UNSUPPORTED, "filter: transform length 2^%d unsupported", p->log2N);
   }
@@ -262,14 +534,34 @@ extern "C" int hr_filter_plan_create(hr_filter_plan** plan, int YL, int ZL, int 
   std::vector<float2> tw(N);
   for (int t = 0; t < N; ++t)
     tw[t] = make_float2((float)std::cos(2.0 * M_PI * t / N), (float)-std::sin(2.0 * M_PI * t / N));
-  hr_filter_plan* p = new hr_filter_plan{YL, ZL, ViewN, log2N, PLC, ZLC, dYL, dZL, SO, nullptr, nullptr};
+  hr_filter_plan* p =
+      new hr_filter_plan{YL, ZL, ViewN, log2N, PLC, ZLC, dYL, dZL, SO, nullptr, nullptr, nullptr, nullptr};
   cudaError_t e = cudaMalloc(&p->d_H, sizeof(float) * N);
   if (e == cudaSuccess) e = cudaMalloc(&p->d_tw, sizeof(float2) * N);
   if (e == cudaSuccess) e = cudaMemcpy(p->d_H, H.data(), sizeof(float) * N, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(p->d_tw, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && N == fft2k::kN) {
+    // the register kernel's tables: W_2048^(j c) by [c][j], W_64^x, the preweight of every sample
+    std::vector<float2> tw2(64 * 32), w64(64);
+    for (int c = 0; c < 64; ++c)
+      for (int j = 0; j < 32; ++j) tw2[c * 32 + j] = tw[(size_t)c * j];
+    for (int x = 0; x < 64; ++x)
+      w64[x] = make_float2((float)std::cos(2.0 * M_PI * x / 64), (float)-std::sin(2.0 * M_PI * x / 64));
+    e = cudaMalloc(&p->d_tw2, sizeof(float2) * tw2.size());
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_wt, sizeof(float) * (size_t)YL * ZL);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_tw2, tw2.data(), sizeof(float2) * tw2.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(fft2k::c_w64, w64.data(), sizeof(float2) * 64);
+    if (e == cudaSuccess) {
+      fft2k::preweight_table_kernel<<<64, 256>>>(p->d_wt, YL, ZL, PLC, ZLC, dYL, dZL, SO);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  }
   if (e != cudaSuccess) {
     cudaFree(p->d_H);
     cudaFree(p->d_tw);
+    cudaFree(p->d_tw2);
+    cudaFree(p->d_wt);
     delete p;
     return hr::fail(e == cudaErrorMemoryAllocation ? HR_ERR_OUT_OF_MEMORY : HR_ERR_CUDA, "filter plan: %s",
                     cudaGetErrorString(e));
@@ -301,5 +593,7 @@ extern "C" void hr_filter_plan_destroy(hr_filter_plan* p) {
   if (!p) return;
   cudaFree(p->d_H);
   cudaFree(p->d_tw);
+  cudaFree(p->d_tw2);
+  cudaFree(p->d_wt);
   delete p;
 }
