@@ -96,6 +96,7 @@ _SIGS = {
     "hr_filter_tc_plan_create": (_i, [ctypes.POINTER(_p), _i, _i, _i] + [_f] * 5),
     "hr_filter_tc_execute": (_i, [_p, _p, _p, _i, _i, _p]),
     "hr_filter_tc_check": (_i, [_p]),
+    "hr_filter_tc_test_stall": (_i, [_p, _i, ctypes.c_uint]),
     "hr_filter_tc_device_bytes": (ctypes.c_size_t, [_p]),
     "hr_filter_tc_plan_destroy": (None, [_p]),
     "hr_recon_check": (_i, [_p]),

@@ -68,11 +68,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 }
 
 // Bounded wait on an mbarrier phase. Returns false (after setting the error
-// flag and the CTA's abort flag) if the phase does not complete in time, or
-// if another role of the CTA has already aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int* err, volatile int* abort_flag) {
+// flag and the CTA's abort flag) if the phase does not complete within
+// `limit` polls, or if another role of the CTA has already aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int* err, volatile int* abort_flag,
+                                          uint32_t limit) {
   const uint32_t addr = smem_u32(bar);
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -87,6 +88,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int* er
   atomicExch(err, 1);
   *abort_flag = 1;
   return false;
+}
+
+// Bounded wait for the completion of a phase whose TMA copies were issued,
+// ignoring the abort flag: a CTA that aborts still lets its own copies land
+// in its shared memory before it exits.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t phase, int* err, uint32_t limit) {
+  const uint32_t addr = smem_u32(bar);
+  for (uint32_t i = 0; i < limit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return;
+  }
+  atomicExch(err, 2);
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
@@ -143,7 +163,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                        const __grid_constant__ CUtensorMap tmA2, const __grid_constant__ CUtensorMap tmT0,
                        const __grid_constant__ CUtensorMap tmT1, const __grid_constant__ CUtensorMap tmT2,
                        uint32_t* __restrict__ out, long long rows, int YL, int n_tiles, int k_blocks,
-                       int* __restrict__ err) {
+                       int* __restrict__ err, int stall_kb, uint32_t wait_limit) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
@@ -176,9 +196,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == 0 && lane == 0) {
     // ---- producer: TMA loads ----------------------------------------------
+    int last_kb[kStages];
+    for (int s = 0; s < kStages; ++s) last_kb[s] = -1;
     for (int kb = 0; kb < k_blocks; ++kb) {
       const int s = kb % kStages;
-      if (kb >= kStages && !mbar_wait(&empty[s], ((kb / kStages) - 1) & 1, err, abort_flag)) break;
+      if (kb >= kStages && !mbar_wait(&empty[s], ((kb / kStages) - 1) & 1, err, abort_flag, wait_limit)) break;
+      if (kb == stall_kb) continue;  // test hook: this block's stage is never filled
+      last_kb[s] = kb;
       uint8_t* st = smem + s * kStageBytes;
       mbar_expect_tx(&full[s], kStageBytes);
       tma_load_2d(st, &tmA0, &full[s], kb * kBK, (int)m0);
@@ -188,11 +212,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       tma_load_2d(st + 3 * kTileA + kTileB, &tmT1, &full[s], kb * kBK, n0);
       tma_load_2d(st + 3 * kTileA + 2 * kTileB, &tmT2, &full[s], kb * kBK, n0);
     }
+    // every issued copy has landed before the CTA can exit (after an abort nobody consumes them)
+    for (int s = 0; s < kStages; ++s)
+      if (last_kb[s] >= 0) mbar_drain(&full[s], (last_kb[s] / kStages) & 1, err, wait_limit);
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----------------------------------------------------------
     for (int kb = 0; kb < k_blocks; ++kb) {
       const int s = kb % kStages;
-      if (!mbar_wait(&full[s], (kb / kStages) & 1, err, abort_flag)) break;
+      if (!mbar_wait(&full[s], (kb / kStages) & 1, err, abort_flag, wait_limit)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint8_t* st = smem + s * kStageBytes;
       const uint64_t a0 = umma_desc_sw128(st), a1 = umma_desc_sw128(st + kTileA),
@@ -217,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncwarp();
 
   // ---- epilogue: TMEM -> BF16 channel pairs --------------------------------
-  const bool waited = mbar_wait(accb, 0, err, abort_flag);
+  const bool waited = mbar_wait(accb, 0, err, abort_flag, wait_limit);
   // tcgen05.ld is warp-collective: the whole warp reads TMEM or none of it does
   const bool acc_ok = __all_sync(0xffffffffu, waited && !*abort_flag);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -360,6 +387,8 @@ struct hr_filter_tc_plan {
   CUtensorMap m_a[kParts], m_t[kParts];
   size_t bytes;
   bool owns_a;  // false: the split parts live in a caller's scratch
+  int stall_kb;          // test hook (hr_filter_tc_test_stall): K block never loaded, -1 normally
+  uint32_t wait_limit;   // polls before a pipeline wait gives up
 };
 
 static void tc_destroy(hr_filter_tc_plan* p) {
@@ -395,6 +424,8 @@ static int tc_create(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float 
   p->YL = YL; p->ZL = ZL; p->ViewN = ViewN; p->PLC = PLC; p->ZLC = ZLC; p->dYL = dYL; p->dZL = dZL; p->SO = SO;
   p->rows = rows;
   p->owns_a = ext == nullptr;
+  p->stall_kb = -1;
+  p->wait_limit = kWaitLimit;
   p->KP = (YL + kBK - 1) / kBK * kBK;
   p->n_tiles = (YL + kBNOut - 1) / kBNOut;
   p->TR = p->n_tiles * kBNOut + (kBN - kBNOut);
@@ -480,7 +511,7 @@ extern "C" int hr_filter_tc_execute(const hr_filter_tc_plan* p, uint32_t* d_pair
   HR_REQUIRE(grid < (1LL << 31), "hr_filter_tc_execute: grid too large");
   toeplitz_tc_kernel<<<(unsigned)grid, kThreads, smem, s>>>(p->m_a[0], p->m_a[1], p->m_a[2], p->m_t[0], p->m_t[1],
                                                            p->m_t[2], d_pairs, p->rows, p->YL, p->n_tiles,
-                                                           p->KP / kBK, p->d_err);
+                                                           p->KP / kBK, p->d_err, p->stall_kb, p->wait_limit);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
 }
@@ -489,7 +520,18 @@ extern "C" int hr_filter_tc_check(const hr_filter_tc_plan* p) {
   HR_REQUIRE(p != nullptr, "hr_filter_tc_check: NULL plan");
   int err = 0;
   HR_CUDA_TRY(cudaMemcpy(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (err) return hr::fail(HR_ERR_CUDA, "tensor-core filter: a pipeline wait timed out (kernel aborted its tile)");
+  if (err) {
+    HR_CUDA_TRY(cudaMemset(p->d_err, 0, sizeof(int)));
+    return hr::fail(HR_ERR_CUDA, "tensor-core filter: a pipeline wait timed out (kernel aborted its tile)");
+  }
+  return HR_OK;
+}
+
+extern "C" int hr_filter_tc_test_stall(hr_filter_tc_plan* p, int k_block, unsigned int wait_polls) {
+  HR_REQUIRE(p != nullptr, "hr_filter_tc_test_stall: NULL plan");
+  HR_REQUIRE(k_block < 0 || wait_polls > 0, "hr_filter_tc_test_stall: wait_polls must be positive");
+  p->stall_kb = k_block < 0 ? -1 : k_block;
+  p->wait_limit = k_block < 0 ? kWaitLimit : (uint32_t)wait_polls;
   return HR_OK;
 }
 

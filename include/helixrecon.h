@@ -161,9 +161,16 @@ int hr_filter_tc_plan_create(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN
                              float dZL, float SO);
 int hr_filter_tc_execute(const hr_filter_tc_plan* plan, uint32_t* d_pairs, const float* d_in, int in_layout,
                          int view0, void* stream);
-/* Reads the plan's device error flag (synchronous): HR_ERR_CUDA if a kernel
- * pipeline wait timed out in an earlier execution. */
+/* Reads and clears the plan's device error flag (synchronous): HR_ERR_CUDA if
+ * a kernel pipeline wait timed out in an earlier execution. */
 int hr_filter_tc_check(const hr_filter_tc_plan* plan);
+/* Test hook, no counterpart in the reference: from the next execution on, the
+ * TMA producer of every CTA leaves K block k_block unloaded (a barrier nothing
+ * completes) and pipeline waits give up after wait_polls polls, so the
+ * bounded-wait abort path runs: the kernel flags the error, lets the copies
+ * it issued land, frees its tensor memory and returns without writing its
+ * tile. k_block < 0 restores normal operation. */
+int hr_filter_tc_test_stall(hr_filter_tc_plan* plan, int k_block, unsigned int wait_polls);
 size_t hr_filter_tc_device_bytes(const hr_filter_tc_plan* plan);
 void hr_filter_tc_plan_destroy(hr_filter_tc_plan* plan);
 
