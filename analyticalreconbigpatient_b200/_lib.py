@@ -132,6 +132,7 @@ _SIGS = {
     "hr_cnn_apply_volume": (_i, [_p, _p, _p, _i, _i, _i, _f, _i, _p]),
     "hr_cnn_pack_input": (_i, [_p, _p, _i, _i, _i, _i, _i, _f, _p]),
     "hr_cnn_check": (_i, [_p]),
+    "hr_cnn_test_stall": (_i, [_p, _i, ctypes.c_uint]),
     "hr_cnn_destroy": (None, [_p]),
     "hr_ge_parse_header": (_i, [_p, ctypes.POINTER(GeHeader)]),
     "hr_ge_read_header": (_i, [ctypes.c_char_p, ctypes.POINTER(GeHeader)]),

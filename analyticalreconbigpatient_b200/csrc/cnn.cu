@@ -79,11 +79,12 @@ __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, ui
 }
 
 // Bounded wait on an mbarrier phase; gives up (returning false) when another
-// role of the CTA has aborted, or after kWaitLimit rounds (then records the
+// role of the CTA has aborted, or after `limit` rounds (then records the
 // error and aborts the CTA).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatile int* abort_flag, int* err) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatile int* abort_flag, int* err,
+                                          uint32_t limit) {
   const uint32_t addr = smem_u32(bar);
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -98,6 +99,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatil
   atomicExch(err, 1);
   *abort_flag = 1;
   return false;
+}
+
+// Bounded wait for a phase the thread itself started (issued TMA copies, or
+// the completion of its own tensor-core operations), ignoring the abort flag:
+// an aborting CTA still lets them finish before it frees TMEM and exits.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t phase, int* err, uint32_t limit) {
+  const uint32_t addr = smem_u32(bar);
+  for (uint32_t i = 0; i < limit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return;
+  }
+  atomicExch(err, 2);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
@@ -182,6 +202,8 @@ struct ConvArgs {
   int B, H, W;
   int rows_per_unit;     // output rows a CTA computes down one 128-pixel column strip
   int* err;
+  int stall_row;         // test hook: the CTA's input row of this index is never loaded (-1: none)
+  uint32_t wait_limit;   // polls before a pipeline wait gives up
 };
 
 // Epilogue of one output row segment: the thread's pixel (b, y, x) with its COUT accumulator values.
@@ -260,7 +282,8 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
   uint64_t* empty = full + kRing;
   uint64_t* tfull = empty + kRing;
   uint64_t* tempty = tfull + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+  uint64_t* mdone = tempty + 2;  // the MMA issuer's last commit (one spare slot keeps 16-byte alignment)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mdone + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   float* bias_s = reinterpret_cast<float*>(tmem_slot + 4);  // 16-byte aligned, COUT floats
 
@@ -278,6 +301,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
       mbar_init(&tfull[s], 1);
       mbar_init(&tempty[s], 128);
     }
+    mbar_init(mdone, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -302,6 +326,8 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
     // ---- producer: input rows of each unit into the ring, G boxes per row --------------------
     if (lane == 0) {
       int h = 0;  // input rows loaded by this CTA
+      int last_h[kRing];
+      for (int s = 0; s < kRing; ++s) last_h[s] = -1;
       bool ok = true;
       for (long long un = blockIdx.x; un < units && ok; un += gridDim.x) {
         const int seg = (int)(un % nseg), chunk = (int)((un / nseg) % nchunk);
@@ -309,15 +335,20 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
         const int y0 = chunk * rpu, ny = min(rpu, a.H - y0);
         for (int j = 0; j < ny + 2; ++j, ++h) {
           const int s = h % kRing;
-          if (h >= kRing && !mbar_wait(&empty[s], ((h / kRing) - 1) & 1, abort_flag, a.err)) {
+          if (h >= kRing && !mbar_wait(&empty[s], ((h / kRing) - 1) & 1, abort_flag, a.err, a.wait_limit)) {
             ok = false;
             break;
           }
+          if (h == a.stall_row) continue;  // test hook: this row's slot is never filled
+          last_h[s] = h;
           mbar_expect_tx(&full[s], kTxBytes);
           for (int g = 0; g < G; ++g)
             tma_load_4d(smem_a + s * kRow + g * kPlane, &a.in_map, &full[s], g * 8, seg * kTileM - 1, y0 - 1 + j, b);
         }
       }
+      // every issued copy lands before the CTA exits (after an abort nobody consumes them)
+      for (int s = 0; s < kRing; ++s)
+        if (last_h[s] >= 0) mbar_drain(&full[s], (last_h[s] / kRing) & 1, a.err, a.wait_limit);
     }
   } else if (warp == 1) {
     // ---- MMA issuer: output row i of a unit reads input rows i, i+1, i+2 of the unit ---------
@@ -330,10 +361,10 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
         for (int i = 0; i < ny && ok; ++i, ++o) {
           for (int j = (i == 0 ? 0 : 2); j < 3 && ok; ++j) {
             const int hh = hbase + i + j;
-            ok = mbar_wait(&full[hh % kRing], (hh / kRing) & 1, abort_flag, a.err);
+            ok = mbar_wait(&full[hh % kRing], (hh / kRing) & 1, abort_flag, a.err, a.wait_limit);
           }
           const int acc = o & 1;
-          if (ok && o >= 2) ok = mbar_wait(&tempty[acc], ((o >> 1) - 1) & 1, abort_flag, a.err);
+          if (ok && o >= 2) ok = mbar_wait(&tempty[acc], ((o >> 1) - 1) & 1, abort_flag, a.err, a.wait_limit);
           if (!ok) break;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
@@ -355,6 +386,9 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
         }
         hbase += ny + 2;
       }
+      // every tensor-core operation issued above completes before TMEM is freed
+      umma_commit(mdone);
+      mbar_drain(mdone, 0, a.err, a.wait_limit);
     }
   } else {
     // ---- epilogue: warps 2-5, TMEM lane quarter warp % 4 --------------------------------------
@@ -367,7 +401,7 @@ __global__ void __launch_bounds__(kThreads) conv_tc_kernel(const __grid_constant
       const int y0 = chunk * rpu, ny = min(rpu, a.H - y0);
       for (int i = 0; i < ny; ++i, ++it) {
         const int acc = it & 1;
-        if (!mbar_wait(&tfull[acc], (it >> 1) & 1, abort_flag, a.err)) {
+        if (!mbar_wait(&tfull[acc], (it >> 1) & 1, abort_flag, a.err, a.wait_limit)) {
           ok = false;
           break;
         }
@@ -555,7 +589,7 @@ int make_act_map(CUtensorMap* map, const void* base, int C, int B, int H, int W)
 // Dynamic shared memory of a conv CTA: input-row ring + weights + barriers + alignment slack.
 template <int CIN, int COUT>
 constexpr size_t conv_smem() {
-  return (size_t)kRing * (CIN / 8) * kPlane + 9 * CIN * COUT * 2 + 256 + COUT * 4 + 128;
+  return (size_t)kRing * (CIN / 8) * kPlane + 9 * CIN * COUT * 2 + 256 + COUT * 4 + 128;  // barriers fit in 256
 }
 
 template <int CIN, int COUT, int EPI>
@@ -620,6 +654,8 @@ struct hr_cnn {
   int* d_err = nullptr;
   long long step = 0;
   size_t bytes = 0;
+  int stall_row = -1;               // test hook (hr_cnn_test_stall)
+  uint32_t wait_limit = kWaitLimit;
 };
 
 namespace {
@@ -676,6 +712,8 @@ ConvArgs base_args(const hr_cnn* n, int B, int H, int W) {
   a.H = H;
   a.W = W;
   a.err = n->d_err;
+  a.stall_row = n->stall_row;
+  a.wait_limit = n->wait_limit;
   return a;
 }
 
@@ -891,7 +929,18 @@ extern "C" int hr_cnn_check(const hr_cnn* n) {
   HR_REQUIRE(n != nullptr, "hr_cnn_check: NULL network");
   int err = 0;
   HR_CUDA_TRY(cudaMemcpy(&err, n->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (err) return hr::fail(HR_ERR_CUDA, "learned correction: a tensor-core wait timed out (kernel aborted)");
+  if (err) {
+    HR_CUDA_TRY(cudaMemset(n->d_err, 0, sizeof(int)));
+    return hr::fail(HR_ERR_CUDA, "learned correction: a tensor-core wait timed out (kernel aborted)");
+  }
+  return HR_OK;
+}
+
+extern "C" int hr_cnn_test_stall(hr_cnn* n, int row, unsigned int wait_polls) {
+  HR_REQUIRE(n != nullptr, "hr_cnn_test_stall: NULL network");
+  HR_REQUIRE(row < 0 || wait_polls > 0, "hr_cnn_test_stall: wait_polls must be positive");
+  n->stall_row = row < 0 ? -1 : row;
+  n->wait_limit = row < 0 ? kWaitLimit : (uint32_t)wait_polls;
   return HR_OK;
 }
 

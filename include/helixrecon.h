@@ -410,7 +410,15 @@ int hr_cnn_apply_volume(hr_cnn* net, float* d_out, const float* d_vol, int XN, i
 /* Network input of slices [z0, z0+nz) of a volume (neighbours clamped at the ends). */
 int hr_cnn_pack_input(uint16_t* d_x, const float* d_vol, int XN, int YN, int ZN, int z0, int nz, float mu_w,
                       void* stream);
+/* Reads and clears the network's device error flag: HR_ERR_CUDA if a
+ * tensor-core pipeline wait timed out in an earlier call. */
 int hr_cnn_check(const hr_cnn* net);
+/* Test hook, no counterpart in the reference: from the next call on, every
+ * conv CTA leaves its input row number `row` unloaded (a barrier nothing
+ * completes) and pipeline waits give up after wait_polls polls; the kernels
+ * flag the error, let their issued copies and tensor-core operations finish,
+ * free their tensor memory and return. row < 0 restores normal operation. */
+int hr_cnn_test_stall(hr_cnn* net, int row, unsigned int wait_polls);
 void hr_cnn_destroy(hr_cnn* net);
 
 /* ---- GE raw data and the segment driver ---------------------------------- */

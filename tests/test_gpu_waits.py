@@ -62,3 +62,41 @@ def test_filter_tc_wait_runs_out_and_device_stays_usable(cuda):
     finally:
         lib.hr_filter_tc_check(plan)
         lib.hr_filter_tc_plan_destroy(plan)
+
+
+def test_cnn_wait_runs_out_and_device_stays_usable(cuda):
+    """The learned correction's conv kernels: every CTA leaves one of its input
+    rows unloaded, so its MMA issuer's wait runs out; forward and training calls
+    return, hr_cnn_check reports (and clears) the timeout, and normal calls
+    afterwards reproduce the results of a run before the stall bit for bit."""
+    from analyticalreconbigpatient_b200 import learned as L
+    from analyticalreconbigpatient_b200.geometry import MU_WATER
+
+    lib = _lib.load()
+    rng = np.random.default_rng(5)
+    B, H, W = 2, 24, 256
+    u = np.zeros((B, H, W, 16), dtype=np.float32)
+    u[..., :5] = rng.standard_normal((B, H, W, 5)).astype(np.float32) * 0.3
+    xb = torch.from_numpy(u).to(cuda).to(torch.bfloat16).view(torch.int16).contiguous()
+    base = torch.full((B, H, W), MU_WATER, device=cuda)
+    from oracle import cnn_oracle as C
+
+    net = L.Corrector(C.init_params(4, zero_last=False), device=cuda)  # a non-zero residual
+    ref = net.forward(xb, base).clone()
+    torch.cuda.synchronize()
+    net.check()
+    _lib.check(lib.hr_cnn_test_stall(net._net, 3, 2000))
+    t = time.perf_counter()
+    net.forward(xb, base)
+    torch.cuda.synchronize()
+    elapsed = time.perf_counter() - t
+    assert lib.hr_cnn_check(net._net) == _lib.HR_ERR_CUDA
+    assert b"timed out" in lib.hr_last_error()
+    assert elapsed < 60.0, elapsed
+    assert lib.hr_cnn_check(net._net) == 0
+    _lib.check(lib.hr_cnn_test_stall(net._net, -1, 0))
+    for _ in range(2):
+        again = net.forward(xb, base).clone()
+        torch.cuda.synchronize()
+        net.check()
+        assert torch.equal(again, ref)
