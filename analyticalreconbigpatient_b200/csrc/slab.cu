@@ -15,11 +15,15 @@
 // scan). The per-slab geometry (first view angle, z offset) lives only in the
 // backprojection tables, so one captured CUDA graph -- rebin, preweight/split,
 // tensor-core filter, backprojection -- serves every slab of a buffer parity.
-// Fan windows are copied into ping-pong buffers on a second stream while the
-// previous slab computes, and each slab's volume leaves its own ping-pong
-// buffer on a third stream while the next slab computes; each slab's tables
-// are built on the host in FP64 and uploaded in stream order before its graph
-// launch. Consecutive slabs' fan windows overlap (by the backprojection window
+// Each slab runs as two captured graphs on two streams: rebin + tensor-core
+// filter (into one of two filtered buffers) on a high-priority stream, and the
+// backprojection on another, so that slab k+1's filter (tensor cores) runs
+// under slab k's backprojection (texture units): the scheduler places the
+// filter's CTAs on SMs as backprojection CTAs retire. Fan windows are copied
+// into ping-pong buffers on a third stream while earlier slabs compute, and
+// each slab's volume leaves its own ping-pong buffer on a fourth stream; each
+// slab's tables are built on the host in FP64 and uploaded in stream order
+// before its backprojection. Consecutive slabs' fan windows overlap (by the backprojection window
 // minus the slab advance, plus the margins): the overlap is copied on the
 // device from the previous window's buffer and only the views a slab adds
 // cross the host link.
@@ -62,12 +66,13 @@ struct hr_slab_plan {
   std::vector<double> w;
   float* d_fan[2] = {nullptr, nullptr};
   float* d_reb = nullptr;
-  uint32_t* d_pairs = nullptr;
+  uint32_t* d_pairs[2] = {nullptr, nullptr};
   float* d_vslab[2] = {nullptr, nullptr};
-  cudaStream_t sc = nullptr, scopy = nullptr, sout = nullptr;
+  // sf: rebin + filter (high priority); sc: backprojection; scopy: fan in; sout: volume out
+  cudaStream_t sf = nullptr, sc = nullptr, scopy = nullptr, sout = nullptr;
   cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
-  cudaEvent_t computed[2] = {nullptr, nullptr}, drained[2] = {nullptr, nullptr};
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaEvent_t filtered[2] = {nullptr, nullptr}, computed[2] = {nullptr, nullptr}, drained[2] = {nullptr, nullptr};
+  cudaGraphExec_t gfilter[2] = {nullptr, nullptr}, gbp[2] = {nullptr, nullptr};
   size_t bytes = 0;
 };
 
@@ -145,19 +150,22 @@ int overlap_views(const SlabLayout& L, const std::vector<int>& mine, int j) {
 void destroy(hr_slab_plan* p) {
   if (!p) return;
   for (int i = 0; i < 2; ++i) {
-    if (p->graph[i]) cudaGraphExecDestroy(p->graph[i]);
+    if (p->gfilter[i]) cudaGraphExecDestroy(p->gfilter[i]);
+    if (p->gbp[i]) cudaGraphExecDestroy(p->gbp[i]);
     hr::bp_fast_destroy(&p->fast[i]);
     cudaFree(p->d_fan[i]);
     cudaFree(p->d_vslab[i]);
+    cudaFree(p->d_pairs[i]);
     if (p->copied[i]) cudaEventDestroy(p->copied[i]);
     if (p->consumed[i]) cudaEventDestroy(p->consumed[i]);
+    if (p->filtered[i]) cudaEventDestroy(p->filtered[i]);
     if (p->computed[i]) cudaEventDestroy(p->computed[i]);
     if (p->drained[i]) cudaEventDestroy(p->drained[i]);
   }
   hr_rebin_plan_destroy(p->rebin);
   hr_filter_tc_plan_destroy(p->ftc);
   cudaFree(p->d_reb);
-  cudaFree(p->d_pairs);
+  if (p->sf) cudaStreamDestroy(p->sf);
   if (p->sc) cudaStreamDestroy(p->sc);
   if (p->scopy) cudaStreamDestroy(p->scopy);
   if (p->sout) cudaStreamDestroy(p->sout);
@@ -204,12 +212,33 @@ int enqueue_fan_copy(hr_slab_plan* p, int j, const float* fan, int fan_view0, bo
   return HR_OK;
 }
 
-// The three stages of one slab on stream s reading fan buffer b (what the
-// graphs capture).
-int slab_kernels(hr_slab_plan* p, int b, cudaStream_t s) {
+// The two halves of one slab for buffer parity b (what the graphs capture):
+// rebin + filter from fan buffer b into filtered buffer b, and the
+// backprojection of filtered buffer b into slab buffer b.
+int slab_filter(hr_slab_plan* p, int b, cudaStream_t s) {
   HR_TRY(hr_rebin_execute(p->rebin, p->d_reb, p->d_fan[b], s));
-  HR_TRY(hr_filter_tc_execute(p->ftc, p->d_pairs, p->d_reb, HR_LAYOUT_REBIN, p->L.margin, s));
-  return hr::bp_fast_execute(p->fast[b], p->gslab, p->d_vslab[b], p->d_pairs, s);
+  return hr_filter_tc_execute(p->ftc, p->d_pairs[b], p->d_reb, HR_LAYOUT_REBIN, p->L.margin, s);
+}
+int slab_bp(hr_slab_plan* p, int b, cudaStream_t s) {
+  return hr::bp_fast_execute(p->fast[b], p->gslab, p->d_vslab[b], p->d_pairs[b], s);
+}
+
+// Captures fn(p, b, s) on stream s into an executable graph.
+int capture(hr_slab_plan* p, int b, cudaStream_t s, int (*fn)(hr_slab_plan*, int, cudaStream_t),
+            cudaGraphExec_t* out) {
+  cudaGraph_t gr = nullptr;
+  HR_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  const int st = fn(p, b, s);
+  const cudaError_t e = cudaStreamEndCapture(s, &gr);
+  if (st != HR_OK) {
+    if (gr) cudaGraphDestroy(gr);
+    return st;
+  }
+  HR_CUDA_TRY(e);
+  const cudaError_t ei = cudaGraphInstantiate(out, gr, 0);
+  cudaGraphDestroy(gr);
+  HR_CUDA_TRY(ei);
+  return HR_OK;
 }
 
 }  // namespace
@@ -286,15 +315,19 @@ extern "C" int hr_slab_plan_create_part(hr_slab_plan** plan, const hr_recon_desc
   for (int b = 0; b < 2 && st == HR_OK; ++b) st = hr::bp_fast_reserve(&p->fast[b], rows, nb, L.Wbp);
   for (int b = 0; b < 2 && st == HR_OK; ++b) st = alloc(p, (void**)&p->d_fan[b], (size_t)L.Wfan * per_view * 4);
   if (st == HR_OK) st = alloc(p, (void**)&p->d_reb, (size_t)L.Wfan * per_view * 4);
-  if (st == HR_OK) st = alloc(p, (void**)&p->d_pairs, (size_t)L.Wbp * per_view * 4);
+  for (int b = 0; b < 2 && st == HR_OK; ++b) st = alloc(p, (void**)&p->d_pairs[b], (size_t)L.Wbp * per_view * 4);
   for (int b = 0; b < 2 && st == HR_OK; ++b) st = alloc(p, (void**)&p->d_vslab[b], (size_t)G.XN * G.YN * L.S * 4);
   if (st == HR_OK) {
-    cudaError_t e = cudaStreamCreateWithFlags(&p->sc, cudaStreamNonBlocking);
+    int prio_lo = 0, prio_hi = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&p->sf, cudaStreamNonBlocking, prio_hi);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->sc, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->scopy, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->sout, cudaStreamNonBlocking);
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
       e = cudaEventCreateWithFlags(&p->copied[b], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->consumed[b], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->filtered[b], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->computed[b], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->drained[b], cudaEventDisableTiming);
     }
@@ -321,27 +354,16 @@ static int prepare(hr_slab_plan* p, const float* fan, int fan_view0, bool fan_on
   hr::BpFastHost h;
   HR_TRY(hr::bp_fast_host_tables(&h, slab_geom(p, k), p->w.data()));
   HR_TRY(hr::bp_fast_upload(&p->fast[b], h, p->sc));
-  HR_TRY(hr_rebin_execute(p->rebin, p->d_reb, p->d_fan[b], p->sc));
-  HR_TRY(hr_filter_tc_execute(p->ftc, p->d_pairs, p->d_reb, HR_LAYOUT_REBIN, p->L.margin, p->sc));
-  HR_TRY(hr::bp_fast_autotune(&p->fast[b], p->gslab, p->d_vslab[b], p->d_pairs, p->sc));
+  HR_TRY(slab_filter(p, b, p->sc));
+  HR_TRY(hr::bp_fast_autotune(&p->fast[b], p->gslab, p->d_vslab[b], p->d_pairs[b], p->sc));
   p->fast[b ^ 1].variant = p->fast[b].variant;
   p->fast[b ^ 1].tuned = p->fast[b].tuned;
   HR_TRY(hr::bp_fast_tex_prepare(&p->fast[b ^ 1], p->gslab));
   HR_CUDA_TRY(cudaStreamSynchronize(p->sc));
   HR_CUDA_TRY(cudaStreamSynchronize(p->scopy));
   for (int bb = 0; bb < 2; ++bb) {
-    cudaGraph_t gr = nullptr;
-    HR_CUDA_TRY(cudaStreamBeginCapture(p->sc, cudaStreamCaptureModeRelaxed));
-    const int st = slab_kernels(p, bb, p->sc);
-    const cudaError_t e = cudaStreamEndCapture(p->sc, &gr);
-    if (st != HR_OK) {
-      if (gr) cudaGraphDestroy(gr);
-      return st;
-    }
-    HR_CUDA_TRY(e);
-    const cudaError_t ei = cudaGraphInstantiate(&p->graph[bb], gr, 0);
-    cudaGraphDestroy(gr);
-    HR_CUDA_TRY(ei);
+    HR_TRY(capture(p, bb, p->sf, slab_filter, &p->gfilter[bb]));
+    HR_TRY(capture(p, bb, p->sc, slab_bp, &p->gbp[bb]));
   }
   if (hr::log_enabled()) {
     char desc[768];
@@ -356,23 +378,28 @@ extern "C" int hr_slab_execute_range(hr_slab_plan* p, float* vol, const float* f
   HR_REQUIRE(p != nullptr && vol != nullptr && fan != nullptr, "hr_slab_execute: NULL argument");
   HR_REQUIRE(fan_view0 >= 0 && fan_view0 <= p->fan_first,
              "hr_slab_execute: fan starts at view %d, the plan reads from view %d", fan_view0, p->fan_first);
-  if (!p->graph[0]) HR_TRY(prepare(p, fan, fan_view0, fan_on_host != 0));
+  if (!p->gbp[0]) HR_TRY(prepare(p, fan, fan_view0, fan_on_host != 0));
   const hr_bp_geom& G = p->d.bp;
   const SlabLayout& L = p->L;
   const int n = (int)p->mine.size();
   HR_TRY(enqueue_fan_copy(p, 0, fan, fan_view0, fan_on_host != 0, true));
   for (int j = 0; j < n; ++j) {
     const int k = p->mine[j], b = j & 1;
-    // tables of slab k: host build (overlaps the previous slab on the GPU), stream-ordered upload
+    // rebin + filter of slab j on the filter stream (under slab j-1's backprojection)
+    HR_CUDA_TRY(cudaStreamWaitEvent(p->sf, p->copied[b], 0));
+    HR_CUDA_TRY(cudaStreamWaitEvent(p->sf, p->computed[b], 0));  // slab j-2's backprojection has read d_pairs[b]
+    HR_CUDA_TRY(cudaGraphLaunch(p->gfilter[b], p->sf));
+    HR_CUDA_TRY(cudaEventRecord(p->consumed[b], p->sf));
+    HR_CUDA_TRY(cudaEventRecord(p->filtered[b], p->sf));
+    if (j + 1 < n) HR_TRY(enqueue_fan_copy(p, j + 1, fan, fan_view0, fan_on_host != 0, true));
+    // tables of slab k: host build (overlaps the GPU), stream-ordered upload, backprojection
     hr::BpFastHost h;
     HR_TRY(hr::bp_fast_host_tables(&h, slab_geom(p, k), p->w.data()));
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->copied[b], 0));
+    HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->filtered[b], 0));
     HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->drained[b], 0));  // slab j-2's volume has left d_vslab[b]
     HR_TRY(hr::bp_fast_upload(&p->fast[b], h, p->sc));
-    HR_CUDA_TRY(cudaGraphLaunch(p->graph[b], p->sc));
-    HR_CUDA_TRY(cudaEventRecord(p->consumed[b], p->sc));
+    HR_CUDA_TRY(cudaGraphLaunch(p->gbp[b], p->sc));
     HR_CUDA_TRY(cudaEventRecord(p->computed[b], p->sc));
-    if (j + 1 < n) HR_TRY(enqueue_fan_copy(p, j + 1, fan, fan_view0, fan_on_host != 0, true));
     // the slab's slices are a strided block of the z-fastest volume; copied out
     // on the output stream while the next slab computes
     const size_t ld = (size_t)G.ZN * 4;
@@ -384,6 +411,7 @@ extern "C" int hr_slab_execute_range(hr_slab_plan* p, float* vol, const float* f
   }
   HR_CUDA_TRY(cudaStreamSynchronize(p->sout));
   HR_CUDA_TRY(cudaStreamSynchronize(p->sc));
+  HR_CUDA_TRY(cudaStreamSynchronize(p->sf));
   HR_CUDA_TRY(cudaStreamSynchronize(p->scopy));
   return hr_filter_tc_check(p->ftc);
 }
@@ -410,7 +438,8 @@ extern "C" int hr_slab_describe(const hr_slab_plan* p, char* buf, int len) {
       snprintf(part, sizeof(part), " (part %d of %d, %s: %d slabs)", p->part, p->nparts,
                p->assign == HR_SLAB_ROUND_ROBIN ? "round robin" : "blocks", (int)p->mine.size());
     snprintf(buf, (size_t)len, "%d slabs of %d slices%s; window %d views (fan %d); graphs %s; backprojection: %s",
-             p->L.nslabs, p->L.S, part, p->L.Wbp, p->L.Wfan, p->graph[0] ? "captured" : "not yet", bp);
+             p->L.nslabs, p->L.S, part, p->L.Wbp, p->L.Wfan,
+             p->gbp[0] ? "captured (filter under backprojection)" : "not yet", bp);
   }
   return HR_OK;
 }
