@@ -202,7 +202,9 @@ int autotune(hr_batch_plan* p) {
   float best = 1e30f;
   int best_v = 0, st = HR_OK;
   for (int v = 0; v < hr::kBatchVariants_n && st == HR_OK; ++v) {
-    if (per_scan(v)) st = set_scan_variants(p, v);  // each scan's own choice (fills inside its launch)
+    // per-scan launches: each scan's own choice (fills inside its launch); texture variants: each scan's
+    // FP16 texture variant (after the per-scan one, a scan may have switched to another copy)
+    if (per_scan(v) || textured(v)) st = set_scan_variants(p, v);
     float ms = 1e30f;
     for (int rep = 0; rep < 2 && st == HR_OK; ++rep) {
       cudaEventRecord(e0, p->sc);

@@ -659,6 +659,47 @@ __global__ void __launch_bounds__(kBx* kBy, MB) bp_tex_batch_kernel(const __grid
   }
 }
 
+// The persistent multi-scan launch with texture taps and code specialised per
+// scan: the work item's scan index selects, by a chain of uniform branches,
+// a copy of the column code that reads scan K's descriptor at a constant
+// index, so its constants stay constant-bank operands as in the single-scan
+// kernel instead of occupying registers for the whole launch.
+template <int NZF, int K>
+__device__ __forceinline__ void tex_item_spec(const BatchParams& B, int sc, int local) {
+  if (sc == K) {
+    const BatchScan& S = B.s[K];
+    const int t = local / S.tiles_x;
+    const int xi = (local - t * S.tiles_x) * kBx + threadIdx.x;
+    const int yi = (t % S.tiles_y) * kBy + threadIdx.y;
+    const int b = t / S.tiles_y;
+    if (xi < S.P.XN && yi < S.P.YN) {
+      if (NZF == 0 && S.nz == 8)
+        tex_column<8>(S.vol, S.X, S.T, S.P, xi, yi, b);
+      else
+        tex_column<NZF == 0 ? 4 : NZF>(S.vol, S.X, S.T, S.P, xi, yi, b);
+    }
+    return;
+  }
+  if constexpr (K + 1 < hr::kBatchMaxScans) tex_item_spec<NZF, K + 1>(B, sc, local);
+}
+
+template <int MB, int NZF>
+__global__ void __launch_bounds__(kBx* kBy, MB) bp_tex_batch_spec_kernel(const __grid_constant__ BatchParams B) {
+  __shared__ int s_item;
+  const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
+  for (;;) {
+    if (leader) s_item = atomicAdd(B.counter, 1);
+    __syncthreads();
+    const int k = s_item;
+    __syncthreads();
+    if (k >= B.count) break;
+    const int item = B.begin + k;
+    int sc = 0;
+    while (sc + 1 < B.n && item >= B.s[sc + 1].item0) ++sc;
+    tex_item_spec<NZF, 0>(B, sc, item - B.s[sc].item0);
+  }
+}
+
 // fp32 [n][YL] rows -> BF16 pairs (u, u+1), round to nearest even.
 __global__ void pack_pairs_kernel(uint32_t* __restrict__ out, const float* __restrict__ in, long long rows, int YL) {
   const long long total = rows * YL;
@@ -1079,6 +1120,20 @@ static int batch_launch_tex(const BatchParams* B, int* ctas, cudaStream_t s) {
   return HR_OK;
 }
 
+template <int MB, int NZF>
+static int batch_launch_spec(const BatchParams* B, int* ctas, cudaStream_t s) {
+  if (ctas) {
+    int per_sm = 0;
+    HR_CUDA_TRY(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_tex_batch_spec_kernel<MB, NZF>, kBx * kBy, 0));
+    *ctas = std::max(per_sm, 1) * sm_count();
+    return HR_OK;
+  }
+  bp_tex_batch_spec_kernel<MB, NZF><<<B->grid, dim3(kBx, kBy), 0, s>>>(*B);
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
 // ctas != nullptr: report the resident CTAs of batch variant bv; else launch *B.
 static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t s) {
   switch (bv) {
@@ -1093,6 +1148,9 @@ static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t 
     case 8: return batch_launch_tex<4, 4>(B, ctas, s);
     case 9: return batch_launch_tex<5, 4>(B, ctas, s);
     case 10: return batch_launch_tex<6, 4>(B, ctas, s);
+    case 12: return batch_launch_spec<1, 0>(B, ctas, s);
+    case 13: return batch_launch_spec<1, 4>(B, ctas, s);
+    case 14: return batch_launch_spec<5, 4>(B, ctas, s);
     case 11:  // per-scan launches: no persistent grid
       if (ctas) {
         *ctas = 0;

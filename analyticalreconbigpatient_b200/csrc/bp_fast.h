@@ -127,16 +127,22 @@ int bp_fast_tex_fill(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, 
 // allow (1: unconstrained; 4; 5; 6), in the gathers issued together (one slice
 // at a time, or chunks of 4 slices) and in the taps (register gathers, or
 // samples of each scan's FP16 texture copy; for these, chunk = 4 runs every
-// scan with 4 slices per thread). The last variant (streams = 1) is not a
+// scan with 4 slices per thread). Variant 11 (streams = 1) is not a
 // persistent launch: every scan runs its own plan's kernel on a stream of its
 // own, forked from and joined back into the batch's stream (the batch plan
-// drives it; bp_fast_batch_execute refuses it).
+// drives it; bp_fast_batch_execute refuses it). Variants 12-14 (spec = 1) are
+// persistent texture launches whose column code is specialised per scan (a
+// constant descriptor index per copy, so each scan's constants are
+// constant-bank operands, not registers): each scan's own slices per thread
+// (12), or 4 for every scan with registers unconstrained (13) or limited for
+// 5 CTAs per SM (14).
 struct BatchVariant {
-  int min_ctas, chunk, tex, streams;
+  int min_ctas, chunk, tex, streams, spec;
 };
 constexpr BatchVariant kBatchVariants[] = {{1, 0}, {5, 0}, {6, 0}, {1, 4}, {5, 4}, {6, 4},
                                            {1, 0, kTexHalf}, {4, 0, kTexHalf}, {4, 4, kTexHalf},
-                                           {5, 4, kTexHalf}, {6, 4, kTexHalf}, {0, 0, 0, 1}};
+                                           {5, 4, kTexHalf}, {6, 4, kTexHalf}, {0, 0, 0, 1},
+                                           {1, 0, kTexHalf, 0, 1}, {1, 4, kTexHalf, 0, 1}, {5, 4, kTexHalf, 0, 1}};
 constexpr int kBatchVariants_n = sizeof(kBatchVariants) / sizeof(kBatchVariants[0]);
 struct BpFastBatchScan {
   const BpFast* f;

@@ -88,6 +88,9 @@ def parse():
     ap.add_argument("--train-steps", type=int, default=2000, help="learned: Adam steps (batch 8)")
     ap.add_argument("--eval-phantoms", type=int, default=100, help="learned: held-out phantoms")
     ap.add_argument("--slab", type=int, default=64, help="slices per slab (bigpatient)")
+    ap.add_argument("--rotations", type=int, default=0,
+                    help="bigpatient: a shorter helix of this many rotations with the same detector, grid and "
+                         "slice thickness (a profiling-size case; 0: the 200-rotation workload)")
     ap.add_argument("--form", choices=["fast", "plain"], default="fast",
                     help="form timed as `value` (the chosen BF16 form by default); the plain FP32 form is "
                          "timed beside it unless --no-plain")
@@ -818,6 +821,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     scan = G.config("full" if args.config in ("batch", "learned") else args.config)
+    if args.config == "bigpatient" and args.rotations > 0:
+        scan = G.replace(scan, rotations=args.rotations, ZN=1)
+        scan = G.replace(scan, ZN=scan.fully_sampled_slices())
     if args.impl == "reference":
         run_reference(args, scan, rank, world)
         return

@@ -357,9 +357,13 @@ int hr_batch_backproject(hr_batch_plan* plan, float* const* d_vols, void* stream
  * for every scan and registers limited for 4, 5 or 6 CTAs per SM (8..10));
  * 11: no persistent launch, every scan's own plan kernel on a stream of its
  * own, forked after the scan's filter (under the next scans' rebinning and
- * filtering) and joined at the end. The gather variants keep the slices per
- * thread each scan's own autotuner chose. Switching variants allocates or
- * frees the scans' texture copies. */
+ * filtering) and joined at the end; 12..14: one persistent launch with FP16
+ * texture taps whose column code is specialised per scan (each scan's
+ * constants read at a fixed descriptor index), each scan's own slices per
+ * thread (12) or 4 for every scan, registers unconstrained (13) or limited
+ * for 5 CTAs per SM (14). The gather variants keep the slices per thread each
+ * scan's own autotuner chose. Switching variants allocates or frees the
+ * scans' texture copies. */
 int hr_batch_select(hr_batch_plan* plan, int variant);
 int hr_batch_describe(const hr_batch_plan* plan, char* buf, int len);
 int hr_batch_check(const hr_batch_plan* plan);
