@@ -43,6 +43,7 @@ struct ViewTab {
 
 struct BpParams {
   int XN, YN, ZN, YL, ZL, PN, N_2pi, half;
+  int qcap;  // longest union view window of a z block of the plain kernel (its weight table rows)
   double XNC, YNC, ZNC, dx, dy, dz, YLC, ZLC, dYL, dZL, h, BetaS, DeltaFai, N_pi, SO, SD, k1;
   double SO2, SOSD, SOSDdZL;
   float k1f, DeltaFaif;
@@ -189,6 +190,109 @@ __global__ void __launch_bounds__(kBx* kBy) bp_plain_kernel(float* __restrict__ 
     if (z0 + m < P.ZN) out[m] = res[m] * P.DeltaFaif;
 }
 
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Plain form with the 3D weight factored (the same split as the fast form):
+//   weight = w1 Gc^k1 / (w2 G^k1 + w1 Gc^k1) = 1 / (1 + Q2(view, slice) E(column, view))
+//   Q2 = (w2 / w1) (|t2| / |t2 -/+ 0.5|)^k1,   E = ((temp1 - UU) / (temp1 + UU))^k1.
+// Each CTA (one z block of NZ slices) first tabulates Q2 for its union view
+// window in shared memory (FP64, -1 where the view is outside the slice's
+// window), so an update costs one table read, one FMA and one reciprocal for
+// its weight instead of two logarithms, an exponential and a division. Index
+// selection (s0, windows, U, V) is unchanged: bit-exact to the reference.
+template <int NZ>
+__global__ void __launch_bounds__(kBx* kBy) bp_plain_q_kernel(float* __restrict__ vol, const float* __restrict__ fp,
+                                                             const ViewTab* __restrict__ views,
+                                                             const float* __restrict__ gw, BpParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* z_s = reinterpret_cast<double*>(smem_raw);        // [NZ] voxel z of the block's slices
+  int* s0_s = reinterpret_cast<int*>(z_s + NZ);             // [NZ] central view
+  int* lo_s = s0_s + NZ;                                     // [NZ] clamped window [lo, hi]
+  int* hi_s = lo_s + NZ;                                     // [NZ]
+  float* w_s = reinterpret_cast<float*>(hi_s + NZ);         // [N_2pi]
+  float* q_s = w_s + P.N_2pi;                                // [qcap][NZ]
+  const int tid = threadIdx.y * kBx + threadIdx.x;
+  const int z0 = blockIdx.z * NZ;
+  for (int t = tid; t < P.N_2pi; t += kBx * kBy) w_s[t] = gw[t];
+  // the block's union window (uniform over the CTA; every thread evaluates it)
+  int pstart = 0x7fffffff, pend = -0x7fffffff;
+#pragma unroll
+  for (int m = 0; m < NZ; ++m) {
+    const ZInfo zi = z_info(P, z0 + m);
+    if (tid == 0) {
+      z_s[m] = zi.z;
+      s0_s[m] = zi.s0;
+      lo_s[m] = zi.lo;
+      hi_s[m] = zi.hi;
+    }
+    pstart = min(pstart, zi.lo);
+    pend = max(pend, zi.hi);
+  }
+  // the host sizes qcap from the same expressions; the clamp only keeps the table in bounds
+  if (pend - pstart + 1 > P.qcap) pend = pstart + P.qcap - 1;
+  __syncthreads();  // w_s and the slice data
+  const int len = pend - pstart + 1;
+  for (int e = tid; e < len * NZ; e += kBx * kBy) {
+    const int q = e / NZ, m = e - q * NZ;
+    const int p = pstart + q;
+    float qv = -1.0f;
+    if (p >= lo_s[m] && p <= hi_s[m]) {
+      const int before = p < s0_s[m];
+      const int d1 = (int)(P.N_pi - (double)(s0_s[m] - p));
+      const int d2 = before ? (int)(d1 + P.N_pi) : (int)(d1 - P.N_pi);
+      const double w1 = w_s[d1], w2 = w_s[d2];
+      const double t2 = __dsub_rn(z_s[m], views[p].hv);
+      const double tc = before ? t2 - 0.5 : t2 + 0.5;
+      qv = w2 == 0.0 ? 0.0f : (float)(w2 / w1 * pow(fabs(t2) / fabs(tc), P.k1));
+    }
+    q_s[e] = qv;
+  }
+  __syncthreads();
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  if (xi >= P.XN || yi >= P.YN) return;
+  const double x = __dmul_rn(__dsub_rn((double)xi, P.XNC), P.dx);
+  const double y = __dmul_rn(__dsub_rn((double)yi, P.YNC), P.dy);
+  float res[NZ];
+#pragma unroll
+  for (int m = 0; m < NZ; ++m) res[m] = 0.0f;
+  const size_t plane = (size_t)P.ZL * P.YL;
+  for (int q = 0; q < len; ++q) {
+    const int p = pstart + q;
+    const ViewTab v = views[p];
+    const ColView cv = col_view(P, x, y, v);
+    if (cv.U <= 0 || cv.U >= P.YL) continue;
+    const float dey = (float)((double)cv.U - cv.U1);
+    const float E = fminf(exp2f(P.k1f * log2f((float)cv.B / (float)cv.A)), 3.0e38f);
+    const float* col = fp + (size_t)p * plane + (cv.U - 1);
+    const float* qrow = q_s + q * NZ;
+#pragma unroll
+    for (int m = 0; m < NZ; ++m) {
+      const float q2 = qrow[m];
+      if (q2 < 0.0f) continue;  // view outside slice m's window (uniform over the CTA)
+      const double temp2 = __dsub_rn(z_s[m], v.hv);
+      double dezd;
+      const int V = row_index(P, cv, temp2, dezd);
+      if (V <= 0 || V >= P.ZL) continue;
+      const float dez = (float)dezd;
+      const float* r0 = col + (size_t)(V - 1) * P.YL;
+      const float* r1 = r0 + P.YL;
+      const float ra = dey * __ldg(r0) + (1.0f - dey) * __ldg(r0 + 1);
+      const float rb = dey * __ldg(r1) + (1.0f - dey) * __ldg(r1 + 1);
+      const float touying = dez * ra + (1.0f - dez) * rb;
+      res[m] += rcp_approx(fmaf(q2, E, 1.0f)) * touying;
+    }
+  }
+  float* out = vol + ((size_t)yi * P.XN + xi) * P.ZN + z0;
+#pragma unroll
+  for (int m = 0; m < NZ; ++m)
+    if (z0 + m < P.ZN) out[m] = res[m] * P.DeltaFaif;
+}
+
 // ---------------------------------------------------------------------------
 // FP64 form: the reference CPU's data path in double on the GPU.
 // ---------------------------------------------------------------------------
@@ -285,7 +389,51 @@ int bp_params_from_geom(const hr_bp_geom* g, const char* who, BpParams* out) {
   P.SOSDdZL = P.SOSD / g->dZL;
   P.k1f = (float)g->k1;
   P.DeltaFaif = (float)g->DeltaFai;
+  // longest union view window of a z block of kNzPlain slices, with the
+  // device's expressions for the central view and the clamped window
+  P.qcap = 0;
+  for (int z0 = 0; z0 < g->ZN; z0 += kNzPlain) {
+    int a = 0x7fffffff, e = -0x7fffffff;
+    for (int zi = z0; zi < z0 + kNzPlain && zi < g->ZN; ++zi) {
+      const double z = (zi - g->ZNC) * g->dz;
+      const double beta0 = kTwoPiTrunc * z / g->h;
+      const int s0 = (int)std::ceil((beta0 - g->BetaS) / g->DeltaFai - 0.5);
+      const int s1 = s0 - half, s2 = s0 + half;
+      if (s1 < g->PN && s2 > 0) {
+        a = std::min(a, s1 < 0 ? 0 : s1);
+        e = std::max(e, s2 > g->PN - 1 ? g->PN - 1 : s2);
+      }
+    }
+    if (e >= a) P.qcap = std::max(P.qcap, e - a + 1);
+  }
   *out = P;
+  return HR_OK;
+}
+
+// Dynamic shared memory of bp_plain_q_kernel.
+size_t plain_q_smem(const BpParams& P) {
+  return sizeof(double) * kNzPlain + 3 * sizeof(int) * kNzPlain + sizeof(float) * P.N_2pi +
+         sizeof(float) * (size_t)P.qcap * kNzPlain;
+}
+// Above this the per-CTA weight table would cost too much occupancy (very
+// thick slices: long union windows); the per-update weight kernel runs instead.
+constexpr size_t kPlainQSmemMax = 96 * 1024;
+
+// The plain-form launch of both the plan and the allocation-free entry (the
+// same kernel for the same geometry, so their results are identical).
+int launch_plain(const BpParams& P, float* vol, const float* fp, const ViewTab* views, const float* w,
+                 cudaStream_t s) {
+  dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, (P.ZN + kNzPlain - 1) / kNzPlain);
+  HR_REQUIRE(grid.z <= 65535 && grid.y <= 65535, "backprojection: grid too large");
+  const size_t qsmem = plain_q_smem(P);
+  if (P.qcap > 0 && qsmem <= kPlainQSmemMax) {
+    HR_CUDA_TRY(cudaFuncSetAttribute(bp_plain_q_kernel<kNzPlain>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)qsmem));
+    bp_plain_q_kernel<kNzPlain><<<grid, dim3(kBx, kBy), qsmem, s>>>(vol, fp, views, w, P);
+  } else {
+    bp_plain_kernel<kNzPlain><<<grid, dim3(kBx, kBy), sizeof(float) * P.N_2pi, s>>>(vol, fp, views, w, P);
+  }
+  HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
 }
 
@@ -357,12 +505,9 @@ extern "C" int hr_bp_execute(const hr_bp_plan* pl, void* d_vol, const void* d_fp
   cudaStream_t s = hr::as_stream(stream);
   if (pl->form == HR_FORM_FAST)
     return hr::bp_fast_execute(pl->fast, pl->fg, static_cast<float*>(d_vol), static_cast<const uint32_t*>(d_fp), s);
-  if (pl->form == HR_FORM_PLAIN) {
-    dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, (P.ZN + kNzPlain - 1) / kNzPlain);
-    HR_REQUIRE(grid.z <= 65535 && grid.y <= 65535, "backprojection: grid too large");
-    bp_plain_kernel<kNzPlain><<<grid, dim3(kBx, kBy), sizeof(float) * P.N_2pi, s>>>(
-        static_cast<float*>(d_vol), static_cast<const float*>(d_fp), pl->d_views, pl->d_w, P);
-  } else {
+  if (pl->form == HR_FORM_PLAIN)
+    return launch_plain(P, static_cast<float*>(d_vol), static_cast<const float*>(d_fp), pl->d_views, pl->d_w, s);
+  {
     dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, (P.ZN + kNzFp64 - 1) / kNzFp64);
     HR_REQUIRE(grid.z <= 65535 && grid.y <= 65535, "backprojection: grid too large");
     bp_fp64_kernel<kNzFp64><<<grid, dim3(kBx, kBy), sizeof(double) * P.N_2pi, s>>>(
@@ -400,8 +545,11 @@ extern "C" int hr_bp_describe(const hr_bp_plan* pl, char* buf, int len) {
   HR_REQUIRE(pl != nullptr, "hr_bp_describe: NULL plan");
   if (pl->form == HR_FORM_FAST) return hr::bp_fast_describe(pl->fast, buf, len);
   if (buf && len > 0)
-    snprintf(buf, (size_t)len, "%s slices_per_thread=%d tile=%dx%d", pl->form == HR_FORM_FP64 ? "fp64" : "plain",
-             pl->form == HR_FORM_FP64 ? kNzFp64 : kNzPlain, kBx, kBy);
+    snprintf(buf, (size_t)len, "%s slices_per_thread=%d tile=%dx%d%s", pl->form == HR_FORM_FP64 ? "fp64" : "plain",
+             pl->form == HR_FORM_FP64 ? kNzFp64 : kNzPlain, kBx, kBy,
+             pl->form == HR_FORM_FP64 ? ""
+             : pl->prm.qcap > 0 && plain_q_smem(pl->prm) <= kPlainQSmemMax ? " weights=per-block table"
+                                                                            : " weights=per update");
   return HR_OK;
 }
 
@@ -477,8 +625,6 @@ extern "C" int hr_bp_plain_noalloc(float* d_vol, const float* d_fp, const float*
              g->PN, kNoAllocMaxViews);
   BpParams P{};
   HR_TRY(bp_params_from_geom(g, "hr_bp_plain_noalloc", &P));
-  dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, (P.ZN + kNzPlain - 1) / kNzPlain);
-  HR_REQUIRE(grid.z <= 65535 && grid.y <= 65535, "hr_bp_plain_noalloc: grid too large");
   cudaStream_t s = hr::as_stream(stream);
   ViewTab* views = nullptr;
   {
@@ -489,7 +635,5 @@ extern "C" int hr_bp_plain_noalloc(float* d_vol, const float* d_fp, const float*
     fill_view_table(g_noalloc_host, P.PN, P.BetaS, P.DeltaFai, P.h);
     HR_CUDA_TRY(cudaMemcpyAsync(views, g_noalloc_host, sizeof(ViewTab) * P.PN, cudaMemcpyHostToDevice, s));
   }
-  bp_plain_kernel<kNzPlain><<<grid, dim3(kBx, kBy), sizeof(float) * P.N_2pi, s>>>(d_vol, d_fp, views, d_w, P);
-  HR_CUDA_TRY(cudaGetLastError());
-  return HR_OK;
+  return launch_plain(P, d_vol, d_fp, views, d_w, s);
 }
