@@ -342,16 +342,20 @@ __global__ void preweight_table_kernel(float* __restrict__ wt, int YL, int ZL, f
 }
 
 template <int IN_LAYOUT>
-__global__ void __launch_bounds__(32 * kWarps, 3) filter2048_kernel(float* __restrict__ out, const float* __restrict__ in,
+__global__ void __launch_bounds__(32 * kWarps, 2) filter2048_kernel(float* __restrict__ out, const float* __restrict__ in,
                                                                 const float* __restrict__ gH,
                                                                 const float2* __restrict__ gtw2,
                                                                 const float* __restrict__ wt, int YL, int ZL,
                                                                 long long rows, int view0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tw2 = reinterpret_cast<float2*>(smem_raw);             // [64][32]
-  float* H = reinterpret_cast<float*>(tw2 + 64 * 32);            // [2048]
+  float2* tw2 = reinterpret_cast<float2*>(smem_raw);             // [64][32]: W^(j c) at [c][j]
+  float2* tw2t = tw2 + 64 * 32;                                  // [32][64]: W^(n c) at [n][c]
+  float* H = reinterpret_cast<float*>(tw2t + 64 * 32);           // [2048]
   float2* xbuf = reinterpret_cast<float2*>(H + kN) + (threadIdx.x >> 5) * (32 * kStride);  // this warp's exchange
-  for (int t = threadIdx.x; t < 64 * 32; t += blockDim.x) tw2[t] = gtw2[t];
+  for (int t = threadIdx.x; t < 64 * 32; t += blockDim.x) {
+    tw2[t] = gtw2[t];
+    tw2t[t] = gtw2[(t & 63) * 32 + (t >> 6)];
+  }
   for (int t = threadIdx.x; t < kN; t += blockDim.x) H[t] = gH[t];
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -386,6 +390,8 @@ __global__ void __launch_bounds__(32 * kWarps, 3) filter2048_kernel(float* __res
       }
       asm volatile("" ::: "memory");  // keep each group's loads next to its use
     }
+    // ---- forward: 64-point DFTs over m, twiddle W_2048^(lane c), exchange ------
+    dft64<false>(v);
     __syncwarp();  // the previous pair's reads of xbuf are done
 #pragma unroll
     for (int k1 = 0; k1 < 8; k1 += 2)
@@ -415,7 +421,7 @@ __global__ void __launch_bounds__(32 * kWarps, 3) filter2048_kernel(float* __res
       dft32_inv(y);
       // ---- twiddle conj(W_2048^(n c)), back into the column ------------------
 #pragma unroll
-      for (int n = 0; n < 32; ++n) xbuf[n * kStride + c] = cmulw<true>(y[n], tw2[c * 32 + n]);
+      for (int n = 0; n < 32; ++n) xbuf[n * kStride + c] = cmulw<true>(y[n], tw2t[n * 64 + c]);
     }
     __syncwarp();
 #pragma unroll
@@ -439,7 +445,9 @@ __global__ void __launch_bounds__(32 * kWarps, 3) filter2048_kernel(float* __res
   }
 }
 
-size_t smem_bytes() { return 64 * 32 * sizeof(float2) + kN * sizeof(float) + kWarps * 32 * kStride * sizeof(float2); }
+size_t smem_bytes() {
+  return 2 * 64 * 32 * sizeof(float2) + kN * sizeof(float) + kWarps * 32 * kStride * sizeof(float2);
+}
 
 template <int IN_LAYOUT>
 int launch(const hr_filter_plan* p, float* out, const float* in, int view0, cudaStream_t s) {

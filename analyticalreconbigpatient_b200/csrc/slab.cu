@@ -358,6 +358,7 @@ static int prepare(hr_slab_plan* p, const float* fan, int fan_view0, bool fan_on
   HR_TRY(hr::bp_fast_autotune(&p->fast[b], p->gslab, p->d_vslab[b], p->d_pairs[b], p->sc));
   p->fast[b ^ 1].variant = p->fast[b].variant;
   p->fast[b ^ 1].tuned = p->fast[b].tuned;
+  std::memcpy(p->fast[b ^ 1].tuned_ms, p->fast[b].tuned_ms, sizeof(p->fast[b].tuned_ms));
   HR_TRY(hr::bp_fast_tex_prepare(&p->fast[b ^ 1], p->gslab));
   HR_CUDA_TRY(cudaStreamSynchronize(p->sc));
   HR_CUDA_TRY(cudaStreamSynchronize(p->scopy));
