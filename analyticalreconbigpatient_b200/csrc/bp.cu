@@ -232,10 +232,13 @@ __global__ void __launch_bounds__(kBx* kBy) bp_plain_q_kernel(float* __restrict_
     pstart = min(pstart, zi.lo);
     pend = max(pend, zi.hi);
   }
-  // the host sizes qcap from the same expressions; the clamp only keeps the table in bounds
-  if (pend - pstart + 1 > P.qcap) pend = pstart + P.qcap - 1;
+  // views of the union window; 0 for a block whose slices all lie outside the
+  // scan (pstart > pend: compared before subtracting, which would overflow).
+  // The host sizes qcap from the same expressions; the clamp only keeps the
+  // table in bounds.
+  int len = pend >= pstart ? pend - pstart + 1 : 0;
+  if (len > P.qcap) len = P.qcap;
   __syncthreads();  // w_s and the slice data
-  const int len = pend - pstart + 1;
   for (int e = tid; e < len * NZ; e += kBx * kBy) {
     const int q = e / NZ, m = e - q * NZ;
     const int p = pstart + q;
