@@ -341,7 +341,13 @@ __global__ void preweight_table_kernel(float* __restrict__ wt, int YL, int ZL, f
   }
 }
 
-template <int IN_LAYOUT>
+// STAGE (rebinning layout, ZL a multiple of 8): a CTA's four warps take the
+// four row pairs of 8 consecutive rows k0..k0+7 of one view; those rows are
+// 32 contiguous bytes per channel, so the CTA first copies the [YL][8] block
+// into shared memory with coalesced 16-byte loads (over the exchange buffers,
+// which are free between pairs) and each warp reads its two rows from there;
+// without staging a lane's load touches a sector of its own.
+template <int IN_LAYOUT, bool STAGE>
 __global__ void __launch_bounds__(32 * kWarps, 2) filter2048_kernel(float* __restrict__ out, const float* __restrict__ in,
                                                                 const float* __restrict__ gH,
                                                                 const float2* __restrict__ gtw2,
@@ -358,10 +364,14 @@ __global__ void __launch_bounds__(32 * kWarps, 2) filter2048_kernel(float* __res
   }
   for (int t = threadIdx.x; t < kN; t += blockDim.x) H[t] = gH[t];
   __syncthreads();
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long pairs = (rows + 1) >> 1;
-  const long long warps = (long long)gridDim.x * kWarps;
-  for (long long pr = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5); pr < pairs; pr += warps) {
+  // STAGE: rows is a multiple of 8, so every tile of kWarps pairs is full and the loop is CTA-uniform
+  const long long first = STAGE ? (long long)blockIdx.x * kWarps : (long long)blockIdx.x * kWarps + warp;
+  const long long step = (long long)gridDim.x * kWarps;
+  float* stage = reinterpret_cast<float*>(H + kN);  // [YL][9] (STAGE), over the exchange buffers
+  for (long long pt = first; pt < pairs; pt += step) {
+    const long long pr = STAGE ? pt + warp : pt;
     const long long ra = 2 * pr, rb = ra + 1;
     const bool hasb = rb < rows;
     const int ka = (int)(ra % ZL), kb = (int)(rb % ZL);
@@ -376,19 +386,52 @@ __global__ void __launch_bounds__(32 * kWarps, 2) filter2048_kernel(float* __res
     const float* wa = wt + (size_t)ka * YL;
     const float* wb = wt + (size_t)kb * YL;
     float2 v[64];
-#pragma unroll
-    for (int m2 = 0; m2 < 8; ++m2) {
-#pragma unroll
-      for (int m1 = 0; m1 < 8; ++m1) {
-        const int n = lane + 32 * (m2 + 8 * m1);
-        float a = 0.0f, b = 0.0f;
-        if (n < YL) {
-          a = __ldg(pa + n * es) * __ldg(wa + n);
-          if (hasb) b = __ldg(pb + n * es) * __ldg(wb + n);
-        }
-        v[m2 + 8 * m1] = make_float2(a, b);
+    if constexpr (STAGE) {
+      // rows 2*pt .. 2*pt+7 are k0 .. k0+7 of view va0 (ZL % 8 == 0)
+      const long long r0 = 2 * pt;
+      const long long va0 = r0 / ZL;
+      const int k0 = (int)(r0 - va0 * ZL);
+      const float4* src = reinterpret_cast<const float4*>(in + (size_t)(view0 + va0) * YL * ZL + k0);
+      __syncthreads();  // every warp has finished reading its exchange buffer (the previous tile)
+      for (int t = threadIdx.x; t < 2 * YL; t += 32 * kWarps) {
+        const int n = t >> 1, hq = t & 1;
+        const float4 q = __ldg(src + (size_t)n * (ZL / 4) + hq);
+        float* d = stage + n * 9 + 4 * hq;
+        d[0] = q.x;
+        d[1] = q.y;
+        d[2] = q.z;
+        d[3] = q.w;
       }
-      asm volatile("" ::: "memory");  // keep each group's loads next to its use
+      __syncthreads();
+#pragma unroll
+      for (int m2 = 0; m2 < 8; ++m2) {
+#pragma unroll
+        for (int m1 = 0; m1 < 8; ++m1) {
+          const int n = lane + 32 * (m2 + 8 * m1);
+          float a = 0.0f, b = 0.0f;
+          if (n < YL) {
+            a = stage[n * 9 + 2 * warp] * __ldg(wa + n);
+            b = stage[n * 9 + 2 * warp + 1] * __ldg(wb + n);
+          }
+          v[m2 + 8 * m1] = make_float2(a, b);
+        }
+      }
+      __syncthreads();  // the staging area is read before any warp writes its exchange buffer
+    } else {
+#pragma unroll
+      for (int m2 = 0; m2 < 8; ++m2) {
+#pragma unroll
+        for (int m1 = 0; m1 < 8; ++m1) {
+          const int n = lane + 32 * (m2 + 8 * m1);
+          float a = 0.0f, b = 0.0f;
+          if (n < YL) {
+            a = __ldg(pa + n * es) * __ldg(wa + n);
+            if (hasb) b = __ldg(pb + n * es) * __ldg(wb + n);
+          }
+          v[m2 + 8 * m1] = make_float2(a, b);
+        }
+        asm volatile("" ::: "memory");  // keep each group's loads next to its use
+      }
     }
     // ---- forward: 64-point DFTs over m, twiddle W_2048^(lane c), exchange ------
     dft64<false>(v);
@@ -449,9 +492,9 @@ size_t smem_bytes() {
   return 2 * 64 * 32 * sizeof(float2) + kN * sizeof(float) + kWarps * 32 * kStride * sizeof(float2);
 }
 
-template <int IN_LAYOUT>
-int launch(const hr_filter_plan* p, float* out, const float* in, int view0, cudaStream_t s) {
-  auto kern = filter2048_kernel<IN_LAYOUT>;
+template <int IN_LAYOUT, bool STAGE>
+int launch_k(const hr_filter_plan* p, float* out, const float* in, int view0, cudaStream_t s) {
+  auto kern = filter2048_kernel<IN_LAYOUT, STAGE>;
   const size_t smem = smem_bytes();
   HR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long rows = (long long)p->ZL * p->ViewN;
@@ -464,6 +507,14 @@ int launch(const hr_filter_plan* p, float* out, const float* in, int view0, cuda
   kern<<<grid, 32 * kWarps, smem, s>>>(out, in, p->d_H, p->d_tw2, p->d_wt, p->YL, p->ZL, rows, view0);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
+}
+
+template <int IN_LAYOUT>
+int launch(const hr_filter_plan* p, float* out, const float* in, int view0, cudaStream_t s) {
+  // staging needs 8-row tiles inside one view and 16-byte aligned channel blocks
+  if constexpr (IN_LAYOUT == HR_LAYOUT_REBIN)
+    if (p->ZL % 8 == 0 && ((uintptr_t)in & 15) == 0) return launch_k<IN_LAYOUT, true>(p, out, in, view0, s);
+  return launch_k<IN_LAYOUT, false>(p, out, in, view0, s);
 }
 
 }  // namespace fft2k
