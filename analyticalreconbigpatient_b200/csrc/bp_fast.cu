@@ -146,6 +146,7 @@ struct ZTabs {
   const uint32_t* zmask;  // per z block and view: slices whose window holds the view
   const int2* zblock;     // per z block: {first view, number of views}
   const int* zoff;        // per z block: table row of its first view
+  const int4* seg;        // per z block: view segments of the segmented texture variants
 };
 
 template <int NZ, int CH, class PT>
@@ -587,15 +588,11 @@ __device__ __forceinline__ void tex_dispatch(float (&res)[NZ], const SegCtx& c, 
     tex_dispatch<NZ, MA + 1, MA + 1>(res, c, P, sg);
 }
 
+// One column of z block b with the segmented view loop (segments in T.seg).
 template <int NZ>
-__global__ void __launch_bounds__(kBx* kBy) bp_tex_seg_kernel(float* __restrict__ vol, const TexRef X, const ZTabs T,
-                                                             const int4* __restrict__ segs, const FastParams P,
-                                                             int b_first) {
+__device__ __forceinline__ void tex_seg_column(float* __restrict__ vol, const TexRef& X, const ZTabs& T,
+                                               const FastParams& P, int xi, int yi, int b) {
   static_assert(NZ % 2 == 0, "table entries are read two slices at a time");
-  const int xi = blockIdx.x * kBx + threadIdx.x;
-  const int yi = blockIdx.y * kBy + threadIdx.y;
-  if (xi >= P.XN || yi >= P.YN) return;
-  const int b = b_first + blockIdx.z;
   const int z0 = b * NZ;
   SegCtx c;
   c.trig = T.trig;
@@ -612,7 +609,7 @@ __global__ void __launch_bounds__(kBx* kBy) bp_tex_seg_kernel(float* __restrict_
   float res[NZ];
 #pragma unroll
   for (int m = 0; m < NZ; ++m) res[m] = 0.0f;
-  const int4* sb = segs + (size_t)b * (hr::kSegPerNz * NZ);
+  const int4* sb = T.seg + (size_t)b * (hr::kSegPerNz * NZ);
 #pragma unroll 1
   for (int sgi = 0; sgi < hr::kSegPerNz * NZ; ++sgi) {
     const int4 sg = __ldg(sb + sgi);
@@ -624,6 +621,15 @@ __global__ void __launch_bounds__(kBx* kBy) bp_tex_seg_kernel(float* __restrict_
 #pragma unroll
   for (int m = 0; m < NZ; ++m)
     if (z0 + m < P.ZN) out[m] = res[m] * outs;
+}
+
+template <int NZ>
+__global__ void __launch_bounds__(kBx* kBy) bp_tex_seg_kernel(float* __restrict__ vol, const TexRef X, const ZTabs T,
+                                                             const FastParams P, int b_first) {
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  if (xi >= P.XN || yi >= P.YN) return;
+  tex_seg_column<NZ>(vol, X, T, P, xi, yi, b_first + blockIdx.z);
 }
 
 // The persistent multi-scan launch with texture taps: the work items and
@@ -697,6 +703,38 @@ __global__ void __launch_bounds__(kBx* kBy, MB) bp_tex_batch_spec_kernel(const _
     int sc = 0;
     while (sc + 1 < B.n && item >= B.s[sc + 1].item0) ++sc;
     tex_item_spec<NZF, 0>(B, sc, item - B.s[sc].item0);
+  }
+}
+
+// The persistent multi-scan launch with the segmented texture column code:
+// work items and their claiming as in bp_tex_batch_kernel; each scan runs the
+// segmented loop over its own view segments with its own slices per thread
+// (8 or 4).
+template <int MB>
+__global__ void __launch_bounds__(kBx* kBy, MB) bp_tex_seg_batch_kernel(const __grid_constant__ BatchParams B) {
+  __shared__ int s_item;
+  const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
+  for (;;) {
+    if (leader) s_item = atomicAdd(B.counter, 1);
+    __syncthreads();
+    const int k = s_item;
+    __syncthreads();
+    if (k >= B.count) break;
+    const int item = B.begin + k;
+    int sc = 0;
+    while (sc + 1 < B.n && item >= B.s[sc + 1].item0) ++sc;
+    const BatchScan& S = B.s[sc];
+    const int local = item - S.item0;
+    const int t = local / S.tiles_x;
+    const int xi = (local - t * S.tiles_x) * kBx + threadIdx.x;
+    const int yi = (t % S.tiles_y) * kBy + threadIdx.y;
+    const int b = t / S.tiles_y;
+    if (xi < S.P.XN && yi < S.P.YN) {
+      if (S.nz == 8)
+        tex_seg_column<8>(S.vol, S.X, S.T, S.P, xi, yi, b);
+      else
+        tex_seg_column<4>(S.vol, S.X, S.T, S.P, xi, yi, b);
+    }
   }
 }
 
@@ -1008,7 +1046,8 @@ static FastParams make_params(const BpFastGeom& g) {
 static TexRef texref(const BpFast& f) { return TexRef{f.tex.d_obj, f.tex.d_scale, f.tex.lsh}; }
 
 static ZTabs ztabs(const BpFastTables& t, const BpFast& f) {
-  return ZTabs{f.d_trig, t.d_tab, t.d_mask, reinterpret_cast<const int2*>(t.d_zblock), t.d_zblock + 2 * t.nblocks};
+  return ZTabs{f.d_trig, t.d_tab, t.d_mask, reinterpret_cast<const int2*>(t.d_zblock), t.d_zblock + 2 * t.nblocks,
+               t.d_seg};
 }
 
 template <int NZ, int CH>
@@ -1029,7 +1068,7 @@ template <int NZ>
 static void launch_tex_seg(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol, int b_first,
                            int b_count, cudaStream_t s) {
   dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
-  bp_tex_seg_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), t.d_seg, P, b_first);
+  bp_tex_seg_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), P, b_first);
 }
 
 // Launches variant v over z blocks [b_first, b_first + b_count) (count < 0: all).
@@ -1134,6 +1173,19 @@ static int batch_launch_spec(const BatchParams* B, int* ctas, cudaStream_t s) {
   return HR_OK;
 }
 
+template <int MB>
+static int batch_launch_seg(const BatchParams* B, int* ctas, cudaStream_t s) {
+  if (ctas) {
+    int per_sm = 0;
+    HR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_tex_seg_batch_kernel<MB>, kBx * kBy, 0));
+    *ctas = std::max(per_sm, 1) * sm_count();
+    return HR_OK;
+  }
+  bp_tex_seg_batch_kernel<MB><<<B->grid, dim3(kBx, kBy), 0, s>>>(*B);
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
 // ctas != nullptr: report the resident CTAs of batch variant bv; else launch *B.
 static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t s) {
   switch (bv) {
@@ -1151,6 +1203,8 @@ static int batch_dispatch(int bv, const BatchParams* B, int* ctas, cudaStream_t 
     case 12: return batch_launch_spec<1, 0>(B, ctas, s);
     case 13: return batch_launch_spec<1, 4>(B, ctas, s);
     case 14: return batch_launch_spec<5, 4>(B, ctas, s);
+    case 15: return batch_launch_seg<1>(B, ctas, s);
+    case 16: return batch_launch_seg<4>(B, ctas, s);
     case 11:  // per-scan launches: no persistent grid
       if (ctas) {
         *ctas = 0;

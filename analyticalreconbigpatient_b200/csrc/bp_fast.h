@@ -135,14 +135,18 @@ int bp_fast_tex_fill(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, 
 // constant descriptor index per copy, so each scan's constants are
 // constant-bank operands, not registers): each scan's own slices per thread
 // (12), or 4 for every scan with registers unconstrained (13) or limited for
-// 5 CTAs per SM (14).
+// 5 CTAs per SM (14). Variants 15-16 (seg = 1) are persistent texture launches
+// running the segmented view loop of the single-scan variants 16-17 with each
+// scan's own slices per thread, registers unconstrained or limited for 4 CTAs
+// per SM.
 struct BatchVariant {
-  int min_ctas, chunk, tex, streams, spec;
+  int min_ctas, chunk, tex, streams, spec, seg;
 };
 constexpr BatchVariant kBatchVariants[] = {{1, 0}, {5, 0}, {6, 0}, {1, 4}, {5, 4}, {6, 4},
                                            {1, 0, kTexHalf}, {4, 0, kTexHalf}, {4, 4, kTexHalf},
                                            {5, 4, kTexHalf}, {6, 4, kTexHalf}, {0, 0, 0, 1},
-                                           {1, 0, kTexHalf, 0, 1}, {1, 4, kTexHalf, 0, 1}, {5, 4, kTexHalf, 0, 1}};
+                                           {1, 0, kTexHalf, 0, 1}, {1, 4, kTexHalf, 0, 1}, {5, 4, kTexHalf, 0, 1},
+                                           {1, 0, kTexHalf, 0, 0, 1}, {4, 0, kTexHalf, 0, 0, 1}};
 constexpr int kBatchVariants_n = sizeof(kBatchVariants) / sizeof(kBatchVariants[0]);
 struct BpFastBatchScan {
   const BpFast* f;

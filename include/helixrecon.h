@@ -361,7 +361,10 @@ int hr_batch_backproject(hr_batch_plan* plan, float* const* d_vols, void* stream
  * texture taps whose column code is specialised per scan (each scan's
  * constants read at a fixed descriptor index), each scan's own slices per
  * thread (12) or 4 for every scan, registers unconstrained (13) or limited
- * for 5 CTAs per SM (14). The gather variants keep the slices per thread each
+ * for 5 CTAs per SM (14); 15..16: one persistent launch running the
+ * segmented view loop of the single-scan variants 16-17 with each scan's own
+ * slices per thread, registers unconstrained (15) or limited for 4 CTAs per
+ * SM (16). The gather variants keep the slices per thread each
  * scan's own autotuner chose. Switching variants allocates or frees the
  * scans' texture copies. */
 int hr_batch_select(hr_batch_plan* plan, int variant);

@@ -55,13 +55,13 @@ def solo(scan, fan, fast_variant):
 NZ_TO_FAST = {16: 0, 8: 3, 4: 8}
 # batch variants with texture taps: the solo FP16 texture variants
 NZ_TO_TEX = {8: 11, 4: 13}
-TEXTURED = (6, 7, 8, 9, 10, 12, 13, 14)
+TEXTURED = (6, 7, 8, 9, 10, 12, 13, 14, 15, 16)
 
 
 PER_SCAN = 11  # each scan's own kernel on a stream of its own
 
 
-@pytest.mark.parametrize("bv", [0, 1, 2, 3, 5, 6, 7, 9, PER_SCAN, 12, 13])
+@pytest.mark.parametrize("bv", [0, 1, 2, 3, 5, 6, 7, 9, PER_SCAN, 12, 13, 15, 16])
 def test_batch_equals_each_scan_alone(cuda, bv):
     scans = uneven_scans()
     fans = fans_for(scans, noise=True)
