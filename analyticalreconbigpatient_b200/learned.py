@@ -234,6 +234,42 @@ def evaluate(net: Corrector, data: PairSet, chunk: int = 8) -> dict:
             "hu_rmse_half_view": math.sqrt(sq_plain / n) / MU_WATER * 1000.0, "slices": n // (H * W)}
 
 
+def error_scales(net: Corrector, data: PairSet, sigma: float = 8.0, chunk: int = 8) -> dict:
+    """Where the remaining error lives: the half-view and the learned errors
+    (against the full-view slices) split into a smooth part (Gaussian blur of
+    sigma pixels, wider than the network's 17 x 17 in-plane receptive field)
+    and the rest, each as an HU RMSE. Error the network cannot see around a
+    pixel shows up in the smooth part."""
+    H, W = data.half.YN, data.half.XN
+    r = int(math.ceil(3 * sigma))
+    g = torch.exp(-0.5 * (torch.arange(-r, r + 1, dtype=torch.float64, device=data.device) / sigma) ** 2)
+    g = (g / g.sum()).float()
+    gx, gy = g.view(1, 1, 1, -1), g.view(1, 1, -1, 1)
+
+    def blur(e):  # e: [n][H][W]
+        e = e.unsqueeze(1)
+        e = torch.nn.functional.conv2d(torch.nn.functional.pad(e, (r, r, 0, 0), mode="replicate"), gx)
+        e = torch.nn.functional.conv2d(torch.nn.functional.pad(e, (0, 0, r, r), mode="replicate"), gy)
+        return e.squeeze(1)
+
+    x = torch.empty((chunk, H, W, 16), dtype=torch.int16, device=data.device)
+    acc = {k: 0.0 for k in ("half_low", "half_high", "learned_low", "learned_high")}
+    n = 0
+    for k in range(len(data)):
+        for z0 in range(0, data.S, chunk):
+            nz = min(chunk, data.S - z0)
+            net.pack_input(x, data.inputs[k], 2 + z0, nz)
+            base = data.inputs[k][:, :, 2 + z0:2 + z0 + nz].permute(2, 0, 1).contiguous()
+            pred = net.forward(x[:nz], base)
+            tgt = data.targets[k][z0:z0 + nz]
+            for name, e in (("half", base - tgt), ("learned", pred - tgt)):
+                lo = blur(e)
+                acc[name + "_low"] += float(torch.sum(lo.double() ** 2))
+                acc[name + "_high"] += float(torch.sum((e - lo).double() ** 2))
+            n += pred.numel()
+    return {f"hu_rmse_{k}": math.sqrt(v / n) / MU_WATER * 1000.0 for k, v in acc.items()} | {"sigma_px": sigma}
+
+
 def main(argv=None) -> None:
     """Train on seeded phantoms and evaluate on held-out ones from the command line:
     python -m analyticalreconbigpatient_b200.learned --phantoms 200 --steps 600 --eval 20 [--save params.npy]"""
@@ -251,6 +287,8 @@ def main(argv=None) -> None:
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--i0", type=float, default=1e5, help="photons per ray before the log (0: noiseless)")
     ap.add_argument("--save", default=None, help="write the trained parameters (.npy)")
+    ap.add_argument("--scales", action="store_true",
+                    help="also split the remaining error into a smooth part and the rest (error_scales)")
     a = ap.parse_args(argv)
     pixel = 0.9766 * 512 / a.grid
     t0 = time.perf_counter()
@@ -263,6 +301,8 @@ def main(argv=None) -> None:
     del train_set
     test_set = PairSet(range(100001, 100001 + a.eval), grid=a.grid, pixel=pixel, I0=a.i0)
     ev = evaluate(net, test_set)
+    if a.scales:
+        ev |= error_scales(net, test_set)
     if a.save:
         np.save(a.save, net.params())
     print(json.dumps({"data_s": t1 - t0, "train_s": t2 - t1, "loss_first": float(np.mean(losses[:20])),
