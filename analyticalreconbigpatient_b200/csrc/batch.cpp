@@ -367,8 +367,9 @@ extern "C" int hr_batch_describe(const hr_batch_plan* p, char* buf, int len) {
                  "%d scans, %lld work items in one persistent launch of %d CTAs (>= %d per SM, taps %s); "
                  "slices per thread by scan:", p->n, hr::bp_fast_batch_items(sc.data(), p->n),
                  p->ctas[p->variant], bv.min_ctas,
-                 bv.tex ? "from FP16 textures" : bv.chunk > 0 ? "gathered in chunks of 4 slices"
-                 : "gathered per slice");
+                 bv.tex ? (bv.seg ? "from FP16 textures, segmented view loop"
+                           : bv.spec ? "from FP16 textures, code specialised per scan" : "from FP16 textures")
+                 : bv.chunk > 0 ? "gathered in chunks of 4 slices" : "gathered per slice");
     for (int i = 0; i < p->n && k > 0 && k < len; ++i) k += snprintf(buf + k, (size_t)(len - k), " %d", sc[i].nz);
   }
   if (k > 0 && k < len)

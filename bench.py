@@ -504,7 +504,8 @@ def run_bigpatient(args, scan, dev, world, rank, barrier, emit=True):
     if bp_ms_per_slice:
         upd_per_slice = updates / scan.ZN
         ach = BYTES_PER_UPDATE_BF16 * upd_per_slice / (bp_ms_per_slice * 1e-3) / 1e9
-        roof = {"bound": "hbm", "kernel": "bp_tex_kernel" if "texture" in desc else "bp_fast_kernel",
+        roof = {"bound": "hbm", "kernel": ("bp_tex_seg_kernel" if "segmented" in desc else "bp_tex_kernel")
+                if "texture" in desc else "bp_fast_kernel",
                 "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": ach / pk["hbm_gbs"], "peak_source": pk_kind, "traffic": None,
                 "note": "gather-equivalent (8 B/update) over the autotuner's best time per slice"}
@@ -632,13 +633,15 @@ def run_batch(args, dev, world, rank, barrier, emit=True):
     n = len(scans)
     if "persistent launch" in desc:
         textured = "FP16 textures" in desc
-        bp_kernel = "bp_tex_batch_kernel" if textured else "bp_fast_batch_kernel"
+        bp_kernel = (("bp_tex_seg_batch_kernel" if "segmented" in desc else "bp_tex_batch_spec_kernel"
+                      if "specialised" in desc else "bp_tex_batch_kernel") if textured else "bp_fast_batch_kernel")
         how = "one persistent backprojection launch"
         bp_launches = 1 + (2 * n if textured else 0)  # + the FP16 scale and fill kernels per scan
     else:
         solo_v = [int(t) for t in desc.split("variant by scan:")[1].split("(")[0].split()]
         n_tex = sum(v >= 11 for v in solo_v)
-        bp_kernel = "bp_tex_kernel" if n_tex else "bp_fast_kernel"
+        bp_kernel = (("bp_tex_seg_kernel" if any(v >= 16 for v in solo_v) else "bp_tex_kernel") if n_tex
+                     else "bp_fast_kernel")
         bp_kernel += " per scan, on parallel streams"
         how = "each scan's backprojection on a stream of its own"
         bp_launches = n + 2 * n_tex
@@ -880,7 +883,8 @@ def main():
     bp_ms = res["stages_ms"]["backprojection"]
     bytes_per_update = BYTES_PER_UPDATE_BF16 if chosen == _lib.HR_FORM_FAST else BYTES_PER_UPDATE_FP32
     textured = chosen == _lib.HR_FORM_FAST and "texture" in res["kernels"]
-    kname = ("bp_tex_kernel" if textured else "bp_fast_kernel") if chosen == _lib.HR_FORM_FAST else "bp_plain_kernel"
+    kname = (("bp_tex_seg_kernel" if "segmented" in res["kernels"] else "bp_tex_kernel") if textured
+             else "bp_fast_kernel") if chosen == _lib.HR_FORM_FAST else "bp_plain_q_kernel"
     achieved = bytes_per_update * updates / (bp_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": pk_kind,
