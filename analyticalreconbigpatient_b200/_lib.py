@@ -144,7 +144,6 @@ _SIGS = {
     "hr_ge_reconstruct": (_i, [ctypes.c_char_p, ctypes.c_char_p, _i, _d, _i, _i, _i, ctypes.POINTER(GeOptions), _i,
                                _p]),
     "hr_accumulate": (_i, [_p, _p, ctypes.c_longlong, _p]),
-    "hr_texture_sample_rate": (_i, [ctypes.POINTER(ctypes.c_double), _p]),
     "hr_recon_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc)]),
     "hr_recon_execute": (_i, [_p, _p, _p, _p]),
     "hr_recon_execute_host": (_i, [_p, _p, _p]),

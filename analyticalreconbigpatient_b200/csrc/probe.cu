@@ -1,7 +1,11 @@
 // Device throughput probe for the texture-sampling backprojection's roofline:
 // the rate at which the texture units return bilinear samples of an FP16
 // layered texture (the format the backprojection samples), measured with CUDA
-// events on a cache-resident texture with every lane active.
+// events on a cache-resident texture with every lane active. Built into a
+// measurement library of its own (libhelixprobe.so), outside the product's C
+// ABI:
+//   int hr_texture_sample_rate(double* samples_per_s, void* stream);
+// synchronises the stream and writes the device-wide bilinear samples per second.
 #include <cuda_fp16.h>
 
 #include <algorithm>

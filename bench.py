@@ -898,12 +898,13 @@ def main():
         # the taps come from the texture units' bilinear filtering (one sample per update), whose
         # rate on this device the library measures; the backprojection time includes filling the
         # layered FP16 copy of the filtered data
-        rate = ctypes.c_double(0.0)
-        _lib.check(_lib.load().hr_texture_sample_rate(ctypes.byref(rate), 0))
+        from analyticalreconbigpatient_b200 import probe
+
+        rate = probe.texture_sample_rate()
         samples = updates / (bp_ms * 1e-3) / 1e9
-        roofline["texture"] = {"achieved": samples, "peak": rate.value / 1e9, "unit": "Gsample/s",
-                               "frac": samples * 1e9 / rate.value if rate.value > 0 else None,
-                               "peak_source": "measured (hr_texture_sample_rate: cache-resident FP16 layered "
+        roofline["texture"] = {"achieved": samples, "peak": rate / 1e9, "unit": "Gsample/s",
+                               "frac": samples * 1e9 / rate if rate > 0 else None,
+                               "peak_source": "measured (libhelixprobe.so hr_texture_sample_rate: cache-resident FP16 layered "
                                               "texture, every lane active)"}
         roofline["note"] = ("gather-equivalent bytes (4 FP16 taps = 8 B per update) / backprojection time "
                             "(texture fill included); the taps are bilinear texture samples, so the bound is the "

@@ -236,13 +236,6 @@ int hr_bp_plain_noalloc(float* d_vol, const float* d_fp, const float* d_w, const
  * backprojection plan reads this layout. */
 int hr_pack_bf16_pairs(uint32_t* d_out, const float* d_in, long long rows, int YL, void* stream);
 
-/* ---- device probe -------------------------------------------------------- */
-/* No counterpart in the reference. Measures the texture units' rate of
- * bilinear samples from an FP16 layered texture (samples per second over the
- * whole device, cache-resident texture, every lane active): the roofline of
- * the texture-sampling backprojection variants. Synchronises the stream. */
-int hr_texture_sample_rate(double* samples_per_s, void* stream);
-
 /* ---- whole chain: rebin -> crop -> preweight/filter -> backprojection ---- */
 /* The per-scan driver of src/analyticalReconBigPatient.m:77-146 as one plan. */
 typedef struct hr_recon_desc {

@@ -183,8 +183,7 @@ def test_texture_sample_rate_probe(cuda):
     """The texture-rate probe (the roofline of the texture variants) returns a
     device-wide bilinear sample rate of the right order for a B200: 148 SMs,
     up to four samples per SM per clock at ~2 GHz."""
-    import ctypes
+    from analyticalreconbigpatient_b200 import probe
 
-    rate = ctypes.c_double(0.0)
-    _lib.check(_lib.load().hr_texture_sample_rate(ctypes.byref(rate), 0))
-    assert 1e11 < rate.value < 4e12, rate.value
+    rate = probe.texture_sample_rate()
+    assert 1e11 < rate < 4e12, rate
