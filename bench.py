@@ -101,9 +101,9 @@ def parse():
                          "otherwise carries as sub-objects")
     ap.add_argument("--extra-steps", type=int, default=5, help="timed steps of each sub-workload")
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--e2e-slab", type=int, default=128,
-                    help="fast form: also time e2e through the slab pipeline with slabs of this many slices "
-                         "(0: off); the faster entry is reported")
+    ap.add_argument("--e2e-slab", default="128,64",
+                    help="fast form: also time e2e through the slab pipeline with slabs of these many slices "
+                         "(comma-separated; empty: off); the fastest entry is reported")
     return ap.parse_args()
 
 
@@ -381,29 +381,33 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
         (e2e_s,) = max_over_ranks([e2e_s], world, dev)
         out["e2e_s"] = e2e_s
         out["e2e_entry"] = "hr_recon_execute_host (C ABI, pinned host buffers)"
-        if fast and args.e2e_slab > 0:
+        slab_sizes = [int(x) for x in str(args.e2e_slab).split(",") if x.strip() and int(x) > 0]
+        if fast and slab_sizes:
             # the same volume through the slab pipeline: host-to-device copies of later slabs' fan windows
             # overlap the reconstruction of earlier slabs (hr_slab_execute with host buffers)
             from analyticalreconbigpatient_b200.pipeline import SlabRecon
 
             rec.close()
             torch.cuda.empty_cache()
-            slab = SlabRecon(scan, slab_slices=args.e2e_slab, device=dev)
-            slab.run(h_fan, h_vol)  # warm (autotunes, captures)
-            barrier()
-            slab_t = []
-            for _ in range(args.e2e_steps):
-                t = time.perf_counter()
-                slab.run(h_fan, h_vol)
-                slab_t.append(time.perf_counter() - t)
-            slab_s = statistics.median(slab_t)
-            (slab_s,) = max_over_ranks([slab_s], world, dev)
             out["e2e_chain_s"] = e2e_s
-            out["e2e_slab_s"] = slab_s
-            slab.close()
-            if slab_s < e2e_s:
-                out["e2e_s"] = slab_s
-                out["e2e_entry"] = f"hr_slab_execute (C ABI, pinned host buffers, z slabs of {args.e2e_slab})"
+            out["e2e_slab_s"] = {}
+            for size in slab_sizes:
+                slab = SlabRecon(scan, slab_slices=size, device=dev)
+                slab.run(h_fan, h_vol)  # warm (autotunes, captures)
+                barrier()
+                slab_t = []
+                for _ in range(args.e2e_steps):
+                    t = time.perf_counter()
+                    slab.run(h_fan, h_vol)
+                    slab_t.append(time.perf_counter() - t)
+                slab_s = statistics.median(slab_t)
+                (slab_s,) = max_over_ranks([slab_s], world, dev)
+                out["e2e_slab_s"][str(size)] = slab_s
+                slab.close()
+                torch.cuda.empty_cache()
+                if slab_s < out["e2e_s"]:
+                    out["e2e_s"] = slab_s
+                    out["e2e_entry"] = f"hr_slab_execute (C ABI, pinned host buffers, z slabs of {size})"
         del h_fan, h_vol
     rec.close()
     torch.cuda.empty_cache()
