@@ -116,6 +116,7 @@ _SIGS = {
     "hr_bp_plain_noalloc": (_i, [_p, _p, _p, ctypes.POINTER(BpGeom), _p]),
     "hr_batch_plan_create": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc), _i]),
     "hr_batch_execute": (_i, [_p, _p, _p, _p]),
+    "hr_batch_execute_host": (_i, [_p, _p, _p]),
     "hr_batch_select": (_i, [_p, _i]),
     "hr_batch_backproject": (_i, [_p, _p, _p]),
     "hr_batch_describe": (_i, [_p, ctypes.c_char_p, _i]),

@@ -36,6 +36,13 @@ struct hr_batch_plan {
   int ctas[hr::kBatchVariants_n] = {};
   float tuned_ms[hr::kBatchVariants_n] = {};
   cudaStream_t sc = nullptr;  // capture stream
+  // host-buffer execution (hr_batch_execute_host), allocated at its first call
+  float* d_stage[2] = {};        // fan staging ring, each the largest scan's fan
+  float* d_hvol = nullptr;       // every scan's volume, at voff[i]
+  std::vector<size_t> voff;
+  cudaStream_t sin = nullptr, sout = nullptr;
+  cudaEvent_t copied[2] = {}, consumed[2] = {}, bp_done = nullptr;
+  bool host_ready = false;
   cudaGraphExec_t graph = nullptr;
   std::vector<const void*> graph_ptrs;
   int graph_variant = -1;
@@ -57,6 +64,15 @@ void destroy(hr_batch_plan* p) {
   for (cudaStream_t q : p->ss) cudaStreamDestroy(q);
   for (cudaEvent_t e : p->ready) cudaEventDestroy(e);
   for (cudaEvent_t e : p->done) cudaEventDestroy(e);
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(p->d_stage[b]);
+    if (p->copied[b]) cudaEventDestroy(p->copied[b]);
+    if (p->consumed[b]) cudaEventDestroy(p->consumed[b]);
+  }
+  cudaFree(p->d_hvol);
+  if (p->bp_done) cudaEventDestroy(p->bp_done);
+  if (p->sin) cudaStreamDestroy(p->sin);
+  if (p->sout) cudaStreamDestroy(p->sout);
   if (p->sc) cudaStreamDestroy(p->sc);
   delete p;
 }
@@ -149,6 +165,46 @@ int enqueue(const hr_batch_plan* p, float* const* vols, const float* const* fans
   }
   if (per_scan(p->variant)) return join_all(p, s);
   return backproject(p, vols, p->variant, s);
+}
+
+size_t fan_elems(const hr_recon_desc& d) { return (size_t)d.YL * d.ZL * d.ViewN; }
+size_t vol_elems(const hr_recon_desc& d) { return (size_t)d.bp.XN * d.bp.YN * d.bp.ZN; }
+
+// Staging for hr_batch_execute_host: two fan buffers (the copy of one scan's
+// fan overlaps the rebinning of the previous one), the volumes, two streams.
+int host_buffers(hr_batch_plan* p) {
+  if (p->host_ready) return HR_OK;
+  size_t nfan_max = 0, vtot = 0;
+  p->voff.assign(p->n, 0);
+  for (int i = 0; i < p->n; ++i) {
+    nfan_max = std::max(nfan_max, fan_elems(p->d[i]));
+    p->voff[i] = vtot;
+    vtot += vol_elems(p->d[i]);
+  }
+  for (int b = 0; b < 2; ++b)
+    if (!p->d_stage[b]) HR_TRY(alloc(p, (void**)&p->d_stage[b], nfan_max * sizeof(float)));
+  if (!p->d_hvol) HR_TRY(alloc(p, (void**)&p->d_hvol, vtot * sizeof(float)));
+  if (!p->sin) HR_CUDA_TRY(cudaStreamCreateWithFlags(&p->sin, cudaStreamNonBlocking));
+  if (!p->sout) HR_CUDA_TRY(cudaStreamCreateWithFlags(&p->sout, cudaStreamNonBlocking));
+  for (int b = 0; b < 2; ++b) {
+    if (!p->copied[b]) HR_CUDA_TRY(cudaEventCreateWithFlags(&p->copied[b], cudaEventDisableTiming));
+    if (!p->consumed[b]) HR_CUDA_TRY(cudaEventCreateWithFlags(&p->consumed[b], cudaEventDisableTiming));
+  }
+  if (!p->bp_done) HR_CUDA_TRY(cudaEventCreateWithFlags(&p->bp_done, cudaEventDisableTiming));
+  p->host_ready = true;
+  return HR_OK;
+}
+
+// The order in which hr_batch_execute_host streams the scans in: the smallest
+// fan first (the first copy overlaps nothing), then the others largest first,
+// so that the last scan, whose compute and copy-out overlap nothing, is small.
+std::vector<int> host_order(const hr_batch_plan* p) {
+  std::vector<int> o(p->n);
+  for (int i = 0; i < p->n; ++i) o[i] = i;
+  std::stable_sort(o.begin(), o.end(),
+                   [p](int a, int b) { return fan_elems(p->d[a]) > fan_elems(p->d[b]); });
+  std::rotate(o.rbegin(), o.rbegin() + 1, o.rend());
+  return o;
 }
 
 // Picks each scan's slices per thread with its own plan's autotuner (the
@@ -333,6 +389,52 @@ extern "C" int hr_batch_execute(hr_batch_plan* p, float* const* d_vols, const fl
   }
   HR_CUDA_TRY(cudaGraphLaunch(p->graph, s));
   return HR_OK;
+}
+
+extern "C" int hr_batch_execute_host(hr_batch_plan* p, float* const* h_vols, const float* const* h_fans) {
+  hr::clear_error();
+  HR_REQUIRE(p != nullptr && h_vols != nullptr && h_fans != nullptr, "hr_batch_execute_host: NULL argument");
+  for (int i = 0; i < p->n; ++i)
+    HR_REQUIRE(h_vols[i] != nullptr && h_fans[i] != nullptr, "hr_batch_execute_host: NULL buffer for scan %d", i);
+  HR_TRY(host_buffers(p));
+  const std::vector<int> order = host_order(p);
+  std::vector<float*> dv(p->n);
+  for (int i = 0; i < p->n; ++i) dv[i] = p->d_hvol + p->voff[i];
+  const bool fork = per_scan(p->variant);
+  cudaStream_t s = p->sc;
+  for (int j = 0; j < p->n; ++j) {
+    const int i = order[j], b = j & 1;
+    // the fan of scan j goes to staging buffer b once scan j-2's rebinning has read it
+    HR_CUDA_TRY(cudaStreamWaitEvent(p->sin, p->consumed[b], 0));
+    HR_CUDA_TRY(cudaMemcpyAsync(p->d_stage[b], h_fans[i], fan_elems(p->d[i]) * sizeof(float),
+                                cudaMemcpyHostToDevice, p->sin));
+    HR_CUDA_TRY(cudaEventRecord(p->copied[b], p->sin));
+    HR_CUDA_TRY(cudaStreamWaitEvent(s, p->copied[b], 0));
+    HR_TRY(hr_rebin_execute(p->rebin[i], p->d_rebinned, p->d_stage[b], s));
+    HR_CUDA_TRY(cudaEventRecord(p->consumed[b], s));
+    HR_TRY(hr_filter_tc_execute(p->ftc[i], p->pairs[i], p->d_rebinned, HR_LAYOUT_REBIN, p->d[i].view0, s));
+    if (fork) {
+      // the scan's backprojection on its own stream, its volume out as soon as it is done
+      HR_TRY(fork_bp(p, i, dv[i], s));
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->done[i], 0));
+      HR_CUDA_TRY(cudaMemcpyAsync(h_vols[i], dv[i], vol_elems(p->d[i]) * sizeof(float), cudaMemcpyDeviceToHost,
+                                  p->sout));
+    }
+  }
+  if (!fork) {
+    HR_TRY(backproject(p, dv.data(), p->variant, s));
+    HR_CUDA_TRY(cudaEventRecord(p->bp_done, s));
+    HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->bp_done, 0));
+    for (int i = 0; i < p->n; ++i)
+      HR_CUDA_TRY(cudaMemcpyAsync(h_vols[i], dv[i], vol_elems(p->d[i]) * sizeof(float), cudaMemcpyDeviceToHost,
+                                  p->sout));
+  } else {
+    HR_TRY(join_all(p, s));
+  }
+  HR_CUDA_TRY(cudaStreamSynchronize(p->sout));
+  HR_CUDA_TRY(cudaStreamSynchronize(s));
+  HR_CUDA_TRY(cudaStreamSynchronize(p->sin));
+  return hr_batch_check(p);
 }
 
 extern "C" int hr_batch_backproject(hr_batch_plan* p, float* const* d_vols, void* stream) {

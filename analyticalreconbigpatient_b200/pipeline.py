@@ -246,6 +246,25 @@ class BatchRecon:
         with torch.cuda.device(self.device):
             _lib.check(_lib.load().hr_batch_execute(self._plan, vp, fp, _stream(self.device, stream)))
 
+    def run_host(self, fans: list[torch.Tensor], volumes: list[torch.Tensor]) -> None:
+        """The batch from host memory, synchronous (hr_batch_execute_host): fans[i]
+        CPU float32 [views][YL][ZL] (page-locked for copies that overlap the
+        computation), volumes[i] CPU float32 [YN][XN][ZN], written in place."""
+        n = len(self.scans)
+        if len(fans) != n or len(volumes) != n:
+            raise ValueError(f"expected {n} fans and volumes")
+        for sc, f, v in zip(self.scans, fans, volumes):
+            if f.is_cuda or v.is_cuda or f.dtype != torch.float32 or v.dtype != torch.float32:
+                raise TypeError("fans and volumes must be CPU float32 tensors")
+            if not (f.is_contiguous() and v.is_contiguous()):
+                raise ValueError("fans and volumes must be contiguous")
+            if tuple(f.shape) != (sc.views, sc.YL, sc.ZL) or tuple(v.shape) != (sc.YN, sc.XN, sc.ZN):
+                raise ValueError("fan or volume shape does not match its scan")
+        fp = (ctypes.c_void_p * n)(*[f.data_ptr() for f in fans])
+        vp = (ctypes.c_void_p * n)(*[v.data_ptr() for v in volumes])
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().hr_batch_execute_host(self._plan, vp, fp))
+
     def backproject(self, volumes: list[torch.Tensor], stream=None) -> None:
         """Only the persistent backprojection, from the filtered data of the last run."""
         vp = (ctypes.c_void_p * len(self.scans))(*[v.data_ptr() for v in volumes])

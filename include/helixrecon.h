@@ -339,6 +339,17 @@ typedef struct hr_batch_plan hr_batch_plan;
 int hr_batch_plan_create(hr_batch_plan** plan, const hr_recon_desc* descs, int n);
 /* d_vols[i]: device [YN][XN][ZN] of scan i; d_fans[i]: device [ViewN][YL][ZL]. */
 int hr_batch_execute(hr_batch_plan* plan, float* const* d_vols, const float* const* d_fans, void* stream);
+/* The same batch from host memory, synchronous: h_fans[i] host [ViewN][YL][ZL],
+ * h_vols[i] host [YN][XN][ZN]. The fans stream in through two device staging
+ * buffers on a copy stream while earlier scans rebin, filter and backproject
+ * (smallest scan first, then the largest ones); with per-scan backprojection
+ * launches (variant 11) each volume is copied out as soon as its scan is done,
+ * otherwise all after the persistent launch. Copies from page-locked host
+ * memory overlap the computation; from pageable memory they are synchronous.
+ * The staging buffers (2 x the largest fan) and the volumes are allocated at
+ * the first call and kept with the plan. Not to be run concurrently with
+ * another call on the same plan. */
+int hr_batch_execute_host(hr_batch_plan* plan, float* const* h_vols, const float* const* h_fans);
 /* Only the persistent backprojection launch, from the filtered data the last
  * hr_batch_execute left in the plan (not captured; for timing the kernel). */
 int hr_batch_backproject(hr_batch_plan* plan, float* const* d_vols, void* stream);

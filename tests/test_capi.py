@@ -63,6 +63,8 @@ def test_argument_validation_precedes_device_use():
     assert st == 1 and b"1..16" in lib.hr_last_error()
     st = lib.hr_batch_plan_create(ctypes.byref(plan), descs, 2)
     assert st == 1 and b"weight table" in lib.hr_last_error()
+    st = lib.hr_batch_execute_host(None, None, None)
+    assert st == 1 and b"hr_batch_execute_host" in lib.hr_last_error()
     st = lib.hr_add_poisson_noise(None, 10, 1e5, 1, None)
     assert st == 1
 

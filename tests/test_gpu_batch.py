@@ -112,6 +112,32 @@ def test_batch_graph_replay_and_new_buffers(cuda):
     rec.close()
 
 
+@pytest.mark.parametrize("bv,pinned", [(PER_SCAN, True), (15, True), (9, False)])
+def test_batch_host_entry_equals_device_entry(cuda, bv, pinned):
+    """hr_batch_execute_host (fans streamed in through the two staging buffers,
+    volumes copied out per scan or after the persistent launch) gives the
+    device entry's volumes bit for bit, from page-locked or pageable memory,
+    and again on a second call (buffers kept with the plan)."""
+    scans = uneven_scans()
+    fans = fans_for(scans, noise=True)
+    rec = BatchRecon(scans)
+    rec.select(bv)
+    vols = [torch.empty((s.YN, s.XN, s.ZN), device=cuda) for s in scans]
+    rec.run(fans, vols)
+    torch.cuda.synchronize()
+    ref = [v.cpu() for v in vols]
+    h_fans = [f.cpu().pin_memory() if pinned else f.cpu() for f in fans]
+    for rep in range(2):
+        h_vols = [torch.full(r.shape, float("nan")).pin_memory() if pinned else torch.full(r.shape, float("nan"))
+                  for r in ref]
+        rec.run_host(h_fans, h_vols)
+        for a, b in zip(h_vols, ref):
+            assert torch.equal(a, b), (bv, rep, rec.describe())
+    with pytest.raises(TypeError):
+        rec.run_host(fans, h_vols)  # device fans
+    rec.close()
+
+
 def test_batch_autotuner_reports_every_variant(cuda):
     rec = BatchRecon(uneven_scans()[:2])
     desc = rec.describe()
