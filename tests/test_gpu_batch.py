@@ -89,12 +89,14 @@ def test_batch_equals_each_scan_alone(cuda, bv):
     rec.close()
 
 
-def test_batch_graph_replay_and_new_buffers(cuda):
+@pytest.mark.parametrize("bv", [3, PER_SCAN])
+def test_batch_graph_replay_and_new_buffers(cuda, bv):
     scans = uneven_scans()[:3]
     fans = fans_for(scans)
     rec = BatchRecon(scans)
+    rec.select(bv)
     desc = rec.describe()
-    assert "3 scans" in desc and "persistent launch" in desc, desc
+    assert "3 scans" in desc and ("persistent launch" in desc) == (bv != PER_SCAN), desc
     vols = [torch.zeros((s.YN, s.XN, s.ZN), device=cuda) for s in scans]
     rec.run(fans, vols)
     first = [v.clone() for v in vols]
