@@ -575,21 +575,83 @@ __device__ __forceinline__ void tex_range(float (&res)[NZ], const SegCtx& c, con
   }
 }
 
-// Runs segment sg = {q0, q1, ma, mb} with the code specialised for its range.
+// Two views per iteration. With thick slices few slices share a view, and one
+// view's few taps in flight per warp leave the texture units waiting on
+// latency; here both views' taps are issued before either is used. Each
+// slice still accumulates view q before view q+1 with the same operations as
+// tex_range, so the bits are the same. A view whose column misses the
+// detector is skipped as there (its per-view values are not used).
 template <int NZ, int MA, int MB>
+__device__ __forceinline__ void tex_range2(float (&res)[NZ], const SegCtx& c, const FastParams& P, int q0, int q1) {
+  int q = q0;
+#pragma unroll 1
+  for (; q + 1 < q1; q += 2) {
+    float tap[2][NZ], qv[2][NZ], E[2];
+    bool onv[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int p = c.blk0 + q + h;
+      const float2 cs = __ldg(c.trig + p);
+      const float UU = -c.x * cs.x - c.y * cs.y;
+      const float Yr = -c.x * cs.y + c.y * cs.x;
+      const float u1 = fmaf(Yr, P.invdYL, P.YLC0);
+      onv[h] = u1 >= 0.0f && u1 < c.utop;  // floor(u1) in [0, YL-2]
+      const float t1sq = P.SO2 - Yr * Yr;
+      const float temp1 = t1sq * rsqrtf(t1sq);
+      const float A = temp1 + UU, B = temp1 - UU;
+      const float K = P.SOSDdZL * rcp_approx(temp1 * A);
+      E[h] = ex2_approx(P.k1 * lg2_approx(B * rcp_approx(A)));
+      const cudaTextureObject_t tx = __ldg(c.texs + (p >> c.lsh));
+      const int layer = p & c.lmask;
+      const float xt = u1 + 0.5f;
+      const float4* e = c.btab + (size_t)(q + h) * (NZ / 2);
+#pragma unroll
+      for (int cc = MA / 2; cc <= MB / 2; ++cc) {
+        const float4 t = __ldg(e + cc);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int m = 2 * cc + i;
+          if (m < MA || m > MB) continue;
+          qv[h][m] = i ? t.w : t.y;
+          const float vh = fmaf(i ? t.z : t.x, K, c.zlch);
+          const bool ok = onv[h] && vh >= 0.5f && vh < c.vtop;
+          tap[h][m] = ok ? tex2DLayered<float>(tx, xt, vh, layer) : 0.0f;
+        }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      if (onv[h]) {
+#pragma unroll
+        for (int m = MA; m <= MB; ++m) res[m] = fmaf(rcp_approx(fmaf(qv[h][m], E[h], 1.0f)), tap[h][m], res[m]);
+      }
+  }
+  if (q < q1) tex_range<NZ, MA, MB>(res, c, P, q, q1);  // an odd last view
+}
+
+// Widest slice range the two-view loop runs (wider ranges: one view at a
+// time, whose taps already fill the texture pipe).
+constexpr int kTwoViewMaxRange = 4;
+
+// Runs segment sg = {q0, q1, ma, mb} with the code specialised for its range
+// (V = 2: two views per iteration for ranges of at most kTwoViewMaxRange slices).
+template <int NZ, int V, int MA, int MB>
 __device__ __forceinline__ void tex_dispatch(float (&res)[NZ], const SegCtx& c, const FastParams& P, int4 sg) {
   if (sg.z == MA && sg.w == MB) {
-    tex_range<NZ, MA, MB>(res, c, P, sg.x, sg.y);
+    if constexpr (V == 2 && MB - MA + 1 <= kTwoViewMaxRange)
+      tex_range2<NZ, MA, MB>(res, c, P, sg.x, sg.y);
+    else
+      tex_range<NZ, MA, MB>(res, c, P, sg.x, sg.y);
     return;
   }
   if constexpr (MB + 1 < NZ)
-    tex_dispatch<NZ, MA, MB + 1>(res, c, P, sg);
+    tex_dispatch<NZ, V, MA, MB + 1>(res, c, P, sg);
   else if constexpr (MA + 1 < NZ)
-    tex_dispatch<NZ, MA + 1, MA + 1>(res, c, P, sg);
+    tex_dispatch<NZ, V, MA + 1, MA + 1>(res, c, P, sg);
 }
 
 // One column of z block b with the segmented view loop (segments in T.seg).
-template <int NZ>
+template <int NZ, int V = 1>
 __device__ __forceinline__ void tex_seg_column(float* __restrict__ vol, const TexRef& X, const ZTabs& T,
                                                const FastParams& P, int xi, int yi, int b) {
   static_assert(NZ % 2 == 0, "table entries are read two slices at a time");
@@ -614,7 +676,7 @@ __device__ __forceinline__ void tex_seg_column(float* __restrict__ vol, const Te
   for (int sgi = 0; sgi < hr::kSegPerNz * NZ; ++sgi) {
     const int4 sg = __ldg(sb + sgi);
     if (sg.x >= sg.y) continue;  // unused entry (uniform over the CTA)
-    tex_dispatch<NZ, 0, 0>(res, c, P, sg);
+    tex_dispatch<NZ, V, 0, 0>(res, c, P, sg);
   }
   const float outs = P.DeltaFai * __ldg(X.scale);
   float* out = vol + ((size_t)yi * P.XN + xi) * P.ZN + z0;
@@ -623,13 +685,13 @@ __device__ __forceinline__ void tex_seg_column(float* __restrict__ vol, const Te
     if (z0 + m < P.ZN) out[m] = res[m] * outs;
 }
 
-template <int NZ>
+template <int NZ, int V>
 __global__ void __launch_bounds__(kBx* kBy) bp_tex_seg_kernel(float* __restrict__ vol, const TexRef X, const ZTabs T,
                                                              const FastParams P, int b_first) {
   const int xi = blockIdx.x * kBx + threadIdx.x;
   const int yi = blockIdx.y * kBy + threadIdx.y;
   if (xi >= P.XN || yi >= P.YN) return;
-  tex_seg_column<NZ>(vol, X, T, P, xi, yi, b_first + blockIdx.z);
+  tex_seg_column<NZ, V>(vol, X, T, P, xi, yi, b_first + blockIdx.z);
 }
 
 // The persistent multi-scan launch with texture taps: the work items and
@@ -1064,11 +1126,11 @@ static void launch_tex(const BpFastTables& t, const BpFast& f, const FastParams&
   bp_tex_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), P, b_first);
 }
 
-template <int NZ>
+template <int NZ, int V>
 static void launch_tex_seg(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol, int b_first,
                            int b_count, cudaStream_t s) {
   dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
-  bp_tex_seg_kernel<NZ><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), P, b_first);
+  bp_tex_seg_kernel<NZ, V><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), P, b_first);
 }
 
 // Launches variant v over z blocks [b_first, b_first + b_count) (count < 0: all).
@@ -1084,10 +1146,13 @@ static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, 
     HR_REQUIRE(f.tex.kind == fv.tex && f.tex.views >= g.PN, "fast backprojection: the textures of variant %d are "
                "not prepared", v);
     if (fv.seg) {
+      const bool two = fv.seg == 2;
       if (kFastNz[fv.table] == 8)
-        launch_tex_seg<8>(t, f, P, vol, b_first, b_count, s);
+        two ? launch_tex_seg<8, 2>(t, f, P, vol, b_first, b_count, s)
+            : launch_tex_seg<8, 1>(t, f, P, vol, b_first, b_count, s);
       else
-        launch_tex_seg<4>(t, f, P, vol, b_first, b_count, s);
+        two ? launch_tex_seg<4, 2>(t, f, P, vol, b_first, b_count, s)
+            : launch_tex_seg<4, 1>(t, f, P, vol, b_first, b_count, s);
     } else {
       switch (kFastNz[fv.table]) {
         case 16: launch_tex<16>(t, f, P, vol, b_first, b_count, s); break;
@@ -1368,7 +1433,8 @@ int bp_fast_describe(const BpFast& f, char* buf, int len) {
   if (!buf || len <= 0) return HR_OK;
   const FastVariant& fv = kFastVariants[f.variant];
   int n = snprintf(buf, (size_t)len, "slices_per_thread=%d gathers=%s tile=%dx%d %s", kFastNz[fv.table],
-                   fv.tex == kTexHalf ? (fv.seg ? "texture-fp16-segmented" : "texture-fp16")
+                   fv.tex == kTexHalf ? (fv.seg == 2 ? "texture-fp16-segmented-two-views"
+                                        : fv.seg ? "texture-fp16-segmented" : "texture-fp16")
                    : fv.tex == kTexFloat ? "texture-fp32"
                    : fv.chunk < 0 ? "paired-f32x2" : fv.chunk == 0 ? "per-slice" : fv.chunk == 4 ? "chunk4" : "chunk8",
                    kBx, kBy, f.tuned == 2 ? "(pinned by HELIXRECON_BP_VARIANT)"

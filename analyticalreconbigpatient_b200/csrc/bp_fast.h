@@ -33,7 +33,9 @@ constexpr int kTexHalf = 1, kTexFloat = 2;
 // a z block runs in segments over which the set of slices whose window holds
 // the view is a fixed range [ma, mb], with code specialised for that range, so
 // slices without the view cost nothing (thick slices: a block's union window
-// is much longer than one slice's).
+// is much longer than one slice's); seg = 2: segments whose range holds at
+// most 4 slices run two views per iteration, both views' taps in flight
+// together (thick slices: few taps per view).
 struct FastVariant {
   int table, chunk, tex, seg;
 };
@@ -41,7 +43,8 @@ constexpr FastVariant kFastVariants[] = {{0, 0}, {0, 4}, {0, 8}, {1, 0}, {1, 4},
                                          {0, -1}, {1, -1}, {2, 0}, {2, -1}, {2, 4},
                                          {1, 0, kTexHalf}, {0, 0, kTexHalf}, {2, 0, kTexHalf},
                                          {1, 0, kTexFloat}, {0, 0, kTexFloat},
-                                         {1, 0, kTexHalf, 1}, {2, 0, kTexHalf, 1}};
+                                         {1, 0, kTexHalf, 1}, {2, 0, kTexHalf, 1},
+                                         {1, 0, kTexHalf, 2}, {2, 0, kTexHalf, 2}};
 constexpr int kFastVariants_n = sizeof(kFastVariants) / sizeof(kFastVariants[0]);
 constexpr int kFastDefaultVariant = 0;
 

@@ -208,7 +208,9 @@ int hr_bp_describe(const hr_bp_plan* plan, char* buf, int len);
  * texture copy of the data with the texture units' bilinear filtering, 14-15
  * eight / sixteen with an FP32 copy, 16-17 eight / four slices per thread
  * from the FP16 copy with the view loop cut into segments of a fixed set of
- * slices holding the view (thick slices); the texture variants allocate the
+ * slices holding the view (thick slices), 18-19 eight / four slices per
+ * thread as 16-17 with two views per iteration in segments of at most four
+ * slices (thick slices: more taps in flight); the texture variants allocate the
  * copy, 2 or 4 bytes per sample, and fill it on every execution).
  * For tests and manual tuning. */
 int hr_bp_select(hr_bp_plan* plan, int variant);

@@ -124,7 +124,7 @@ def test_every_fast_variant_gives_the_same_volume(cuda, pixel):
     fast.pack(pairs, filt)
     lib = _lib.load()
     vols = []
-    nvar = 18
+    nvar = 20
     for v in range(nvar):
         _lib.check(lib.hr_bp_select(fast._bp, v))
         vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
@@ -145,9 +145,40 @@ def test_every_fast_variant_gives_the_same_volume(cuda, pixel):
         assert rel_l2(vols[v], vols[0]) < 1e-2, (v, rel_l2(vols[v], vols[0]))
     assert np.array_equal(vols[11], vols[12]) and np.array_equal(vols[11], vols[13])
     assert np.array_equal(vols[14], vols[15])
-    # segmented view loops (16: 8 slices per thread, 17: 4): same operations per slice and view
+    # segmented view loops (16: 8 slices per thread, 17: 4; 18, 19: two views per iteration in narrow
+    # segments): same operations per slice and view, in the same order
     assert np.array_equal(vols[16], vols[11]) and np.array_equal(vols[17], vols[13])
+    assert np.array_equal(vols[18], vols[11]) and np.array_equal(vols[19], vols[13])
     assert np.isfinite(vols[0]).all()
+
+
+def test_two_view_segments_equal_one_view_at_thick_slices(cuda):
+    """At 4 mm slices most segments hold a few slices, so the two-view loop of
+    variants 18-19 (8 / 4 slices per thread) runs for most views (odd segment
+    lengths included); it must give the one-view loop's bits (variants 16-17
+    and 11 / 13, the same operations per slice and view in the same order)."""
+    from analyticalreconbigpatient_b200.pipeline import StagePlans
+
+    sc = G.Scan(ZL=16, pitch=0.9375, rotations=4, XN=48, YN=40, ZN=1, dx=0.98, dy=0.98, dz=4.0)
+    sc = G.replace(sc, ZN=sc.fully_sampled_slices())
+    assert sc.ZN >= 8, sc.ZN
+    rng = np.random.default_rng(5)
+    filt = torch.tensor(rng.standard_normal((sc.PN, sc.ZL, sc.YL)).astype(np.float32), device=cuda)
+    fast = StagePlans(sc, _lib.HR_FORM_FAST)
+    pairs = torch.empty((sc.PN, sc.ZL, sc.YL), dtype=torch.int32, device=cuda)
+    fast.pack(pairs, filt)
+    lib = _lib.load()
+    vols = {}
+    for v in (11, 13, 16, 17, 18, 19):
+        _lib.check(lib.hr_bp_select(fast._bp, v))
+        vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
+        fast.backproject(vol, pairs)
+        torch.cuda.synchronize()
+        vols[v] = vol.cpu().numpy()
+    fast.close()
+    assert np.isfinite(vols[11]).all() and np.count_nonzero(vols[11]) > vols[11].size // 2
+    for a, b in ((18, 11), (16, 11), (19, 13), (17, 13)):
+        assert np.array_equal(vols[a], vols[b]), (a, b)
 
 
 @pytest.mark.parametrize("gain", [2.0**18, 2.0**-100])
