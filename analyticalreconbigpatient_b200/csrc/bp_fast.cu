@@ -1346,12 +1346,6 @@ int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint
   return run_variant(f, g, f.variant, vol, fpb, 0, -1, s);
 }
 
-int bp_fast_execute_filled(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s) {
-  return run_variant(f, g, f.variant, vol, fpb, 0, -1, s);
-}
-
-bool bp_fast_textured(const BpFast& f) { return kFastVariants[f.variant].tex != 0; }
-
 // HELIXRECON_BP_VARIANT=<index> pins the variant and skips the timing (for
 // profiling runs, whose serialised launches would skew the choice, and for
 // reproducible benchmarks).

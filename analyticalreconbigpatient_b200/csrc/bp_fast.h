@@ -116,11 +116,6 @@ int bp_fast_reserve(BpFast* f, const size_t rows[kFastTableSets], const int nblo
 int bp_fast_upload(BpFast* f, const BpFastHost& h, cudaStream_t s);
 void bp_fast_destroy(BpFast* f);
 int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s);
-// bp_fast_execute without the texture fill: for callers that fill the plan's
-// layered copy themselves (bp_fast_tex_fill) earlier in stream order.
-int bp_fast_execute_filled(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s);
-// True when the plan's variant samples a layered texture copy.
-bool bp_fast_textured(const BpFast& f);
 int bp_fast_autotune(BpFast* f, const BpFastGeom& g, float* vol, const uint32_t* fpb, cudaStream_t s);
 int bp_fast_describe(const BpFast& f, char* buf, int len);
 // Allocates (or frees) the layered textures the plan's variant samples

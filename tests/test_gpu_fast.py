@@ -159,7 +159,7 @@ def test_two_view_segments_equal_one_view_at_thick_slices(cuda):
     and 11 / 13, the same operations per slice and view in the same order)."""
     from analyticalreconbigpatient_b200.pipeline import StagePlans
 
-    sc = G.Scan(ZL=16, pitch=0.9375, rotations=4, XN=48, YN=40, ZN=1, dx=0.98, dy=0.98, dz=4.0)
+    sc = G.Scan(ZL=16, pitch=0.9375, rotations=6, XN=48, YN=40, ZN=1, dx=0.98, dy=0.98, dz=4.0)
     sc = G.replace(sc, ZN=sc.fully_sampled_slices())
     assert sc.ZN >= 8, sc.ZN
     rng = np.random.default_rng(5)
