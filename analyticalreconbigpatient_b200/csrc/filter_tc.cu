@@ -33,6 +33,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -279,52 +280,67 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
-// Preweight + split into K-major BF16 rows. Tile of 32 channels x 32 rows k
+// Preweight + split into K-major BF16 rows. Tile of 64 channels x 32 rows k
 // of one view, transposed through shared memory: reads are contiguous along
-// k (rebin layout) or j (row layout), writes along j.
+// k (rebin layout) or j (row layout); each thread writes two adjacent
+// channels of a row as one 32-bit word per part (128 bytes per warp). The
+// CTA strides over the views (grid z may be smaller than the view count).
 template <int IN_LAYOUT>
-__global__ void __launch_bounds__(256) prep_split_kernel(__nv_bfloat16* __restrict__ a0,
-                                                         __nv_bfloat16* __restrict__ a1,
-                                                         __nv_bfloat16* __restrict__ a2,
+__global__ void __launch_bounds__(256) prep_split_kernel(__nv_bfloat162* __restrict__ a0,
+                                                         __nv_bfloat162* __restrict__ a1,
+                                                         __nv_bfloat162* __restrict__ a2,
                                                          const float* __restrict__ in, int YL, int ZL, int KP,
-                                                         int view0, float PLC, float ZLC, float dYL, float dZL,
-                                                         float SO) {
-  __shared__ float tile[32][33];
-  const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
-  const long long v = blockIdx.z;
+                                                         int nviews, int view0, float PLC, float ZLC, float dYL,
+                                                         float dZL, float SO) {
+  __shared__ float tile[64][33];  // [j][k]
+  const int j0 = blockIdx.x * 64, k0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   const float SO2 = SO * SO;
-  for (int yy = ty; yy < 32; yy += 8) {
-    float val = 0.0f;
+  for (long long v = blockIdx.z; v < nviews; v += gridDim.z) {  // uniform over the CTA
+    if (v != blockIdx.z) __syncthreads();                        // the previous view's tile has been read
     if (IN_LAYOUT == HR_LAYOUT_REBIN) {
-      const int j = j0 + yy, k = k0 + tx;
-      if (j < YL && k < ZL) val = in[((size_t)(view0 + v) * YL + j) * ZL + k];
-      tile[yy][tx] = val;  // [j][k]
+      for (int yy = ty; yy < 64; yy += 8) {
+        const int j = j0 + yy, k = k0 + tx;
+        tile[yy][tx] = (j < YL && k < ZL) ? in[((size_t)(view0 + v) * YL + j) * ZL + k] : 0.0f;
+      }
     } else {
-      const int k = k0 + yy, j = j0 + tx;
-      if (j < YL && k < ZL) val = in[((size_t)(view0 + v) * ZL + k) * YL + j];
-      tile[tx][yy] = val;  // [j][k]
+      for (int yy = ty; yy < 32; yy += 8) {
+        const int k = k0 + yy;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = j0 + tx + 32 * h;
+          tile[tx + 32 * h][yy] = (j < YL && k < ZL) ? in[((size_t)(view0 + v) * ZL + k) * YL + j] : 0.0f;
+        }
+      }
     }
-  }
-  __syncthreads();
-  for (int yy = ty; yy < 32; yy += 8) {
-    const int k = k0 + yy, j = j0 + tx;
-    if (k >= ZL || j >= KP) continue;
-    float x = 0.0f;
-    if (j < YL) {
-      const float t = ((float)j - PLC) * dYL;
+    __syncthreads();
+    for (int yy = ty; yy < 32; yy += 8) {
+      const int k = k0 + yy, j = j0 + 2 * tx;
+      if (k >= ZL || j >= KP) continue;  // KP is a multiple of 64: j + 1 < KP too
       const float b = ((float)k - ZLC) * dZL;
-      const float wei = SO2 / sqrtf(SO2 * (SO2 + b * b) - b * t * b * t);
-      x = tile[tx][yy] * wei;
+      float x[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        x[h] = 0.0f;
+        if (j + h < YL) {
+          const float t = ((float)(j + h) - PLC) * dYL;
+          const float wei = SO2 / sqrtf(SO2 * (SO2 + b * b) - b * t * b * t);
+          x[h] = tile[2 * tx + h][yy] * wei;
+        }
+      }
+      __nv_bfloat16 p0[2], p1[2], p2[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        p0[h] = __float2bfloat16_rn(x[h]);
+        const float r1 = x[h] - __bfloat162float(p0[h]);
+        p1[h] = __float2bfloat16_rn(r1);
+        p2[h] = __float2bfloat16_rn(r1 - __bfloat162float(p1[h]));
+      }
+      const size_t o = (((size_t)v * ZL + k) * KP + j) >> 1;
+      a0[o] = __halves2bfloat162(p0[0], p0[1]);
+      a1[o] = __halves2bfloat162(p1[0], p1[1]);
+      a2[o] = __halves2bfloat162(p2[0], p2[1]);
     }
-    const __nv_bfloat16 p0 = __float2bfloat16_rn(x);
-    const float r1 = x - __bfloat162float(p0);
-    const __nv_bfloat16 p1 = __float2bfloat16_rn(r1);
-    const __nv_bfloat16 p2 = __float2bfloat16_rn(r1 - __bfloat162float(p1));
-    const size_t o = ((size_t)v * ZL + k) * KP + j;
-    a0[o] = p0;
-    a1[o] = p1;
-    a2[o] = p2;
   }
 }
 
@@ -487,22 +503,27 @@ extern "C" int hr_filter_tc_plan_create(hr_filter_tc_plan** plan, int YL, int ZL
   return tc_create(plan, YL, ZL, ViewN, PLC, ZLC, dYL, dZL, SO, nullptr);
 }
 
-extern "C" int hr_filter_tc_execute(const hr_filter_tc_plan* p, uint32_t* d_pairs, const float* d_in, int in_layout,
-                                    int view0, void* stream) {
+int hr::filter_tc_execute_limited(const hr_filter_tc_plan* p, uint32_t* d_pairs, const float* d_in, int in_layout,
+                                  int view0, int max_prep_ctas, cudaStream_t s) {
   HR_REQUIRE(p != nullptr && d_pairs != nullptr && d_in != nullptr, "hr_filter_tc_execute: NULL argument");
   HR_REQUIRE(view0 >= 0, "hr_filter_tc_execute: view0 < 0");
   HR_REQUIRE(in_layout == HR_LAYOUT_ROWS || in_layout == HR_LAYOUT_REBIN, "hr_filter_tc_execute: unknown layout %d",
              in_layout);
   HR_REQUIRE(((uintptr_t)d_pairs & 15) == 0, "hr_filter_tc_execute: output must be 16-byte aligned");
-  cudaStream_t s = hr::as_stream(stream);
-  dim3 pgrid(p->KP / 32, (p->ZL + 31) / 32, p->ViewN);
   HR_REQUIRE(p->ViewN <= 65535, "hr_filter_tc_execute: %d views exceed one launch (65535)", p->ViewN);
+  const int gxy = (p->KP / 64) * ((p->ZL + 31) / 32);
+  int gz = p->ViewN;  // the prep kernel strides over the views
+  if (max_prep_ctas > 0) gz = std::max(1, std::min(gz, max_prep_ctas / gxy));
+  const dim3 pgrid(p->KP / 64, (p->ZL + 31) / 32, gz);
+  auto* a0 = reinterpret_cast<__nv_bfloat162*>(p->d_a[0]);
+  auto* a1 = reinterpret_cast<__nv_bfloat162*>(p->d_a[1]);
+  auto* a2 = reinterpret_cast<__nv_bfloat162*>(p->d_a[2]);
   if (in_layout == HR_LAYOUT_REBIN)
-    prep_split_kernel<HR_LAYOUT_REBIN><<<pgrid, 256, 0, s>>>(p->d_a[0], p->d_a[1], p->d_a[2], d_in, p->YL, p->ZL,
-                                                             p->KP, view0, p->PLC, p->ZLC, p->dYL, p->dZL, p->SO);
+    prep_split_kernel<HR_LAYOUT_REBIN><<<pgrid, 256, 0, s>>>(a0, a1, a2, d_in, p->YL, p->ZL, p->KP, p->ViewN, view0,
+                                                             p->PLC, p->ZLC, p->dYL, p->dZL, p->SO);
   else
-    prep_split_kernel<HR_LAYOUT_ROWS><<<pgrid, 256, 0, s>>>(p->d_a[0], p->d_a[1], p->d_a[2], d_in, p->YL, p->ZL,
-                                                            p->KP, view0, p->PLC, p->ZLC, p->dYL, p->dZL, p->SO);
+    prep_split_kernel<HR_LAYOUT_ROWS><<<pgrid, 256, 0, s>>>(a0, a1, a2, d_in, p->YL, p->ZL, p->KP, p->ViewN, view0,
+                                                            p->PLC, p->ZLC, p->dYL, p->dZL, p->SO);
   HR_CUDA_TRY(cudaGetLastError());
   const size_t smem = (size_t)kStages * kStageBytes + 1024 + 128;
   HR_CUDA_TRY(cudaFuncSetAttribute(toeplitz_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -514,6 +535,11 @@ extern "C" int hr_filter_tc_execute(const hr_filter_tc_plan* p, uint32_t* d_pair
                                                            p->KP / kBK, p->d_err, p->stall_kb, p->wait_limit);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
+}
+
+extern "C" int hr_filter_tc_execute(const hr_filter_tc_plan* p, uint32_t* d_pairs, const float* d_in, int in_layout,
+                                    int view0, void* stream) {
+  return hr::filter_tc_execute_limited(p, d_pairs, d_in, in_layout, view0, 0, hr::as_stream(stream));
 }
 
 extern "C" int hr_filter_tc_check(const hr_filter_tc_plan* p) {

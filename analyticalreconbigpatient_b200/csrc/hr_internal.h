@@ -75,4 +75,11 @@ size_t filter_tc_scratch_bytes(int YL, int ZL, int ViewN);
 int filter_tc_create_shared(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC, float dYL,
                             float dZL, float SO, void* const scratch[3]);
 
+// Launches with a bounded number of CTAs (max_ctas <= 0: one CTA per tile, as
+// the public entries): memory-bound stages that run beside a texture-bound
+// backprojection leave it most of the SMs' CTA slots.
+int rebin_execute_limited(const hr_rebin_plan* p, float* d_out, const float* d_proj, int max_ctas, cudaStream_t s);
+int filter_tc_execute_limited(const hr_filter_tc_plan* p, uint32_t* d_pairs, const float* d_in, int in_layout,
+                              int view0, int max_prep_ctas, cudaStream_t s);
+
 }  // namespace hr

@@ -22,6 +22,7 @@
 // contiguous, so a thread moves 4 rows at once (16-byte loads/stores) and the
 // four taps of a warp are contiguous runs. Grid: x over (channel, row quad),
 // y over views (grid-stride beyond 65535).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -112,6 +113,94 @@ __global__ void __launch_bounds__(256) rebin_kernel(float* __restrict__ out, con
   }
 }
 
+// Packed FP32x2 arithmetic (one instruction for two lanes; each lane rounded
+// to nearest like the scalar mul.rn / add.rn, no contraction).
+__device__ __forceinline__ unsigned long long pack2(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+// blend4 on a pair of rows.
+__device__ __forceinline__ unsigned long long blend2(unsigned long long wbb, unsigned long long wub,
+                                                     unsigned long long wbu, unsigned long long wuu,
+                                                     unsigned long long a, unsigned long long b,
+                                                     unsigned long long c, unsigned long long d) {
+  unsigned long long acc = mul2(wbb, a);
+  acc = add2(acc, mul2(wub, b));
+  acc = add2(acc, mul2(wbu, c));
+  return add2(acc, mul2(wuu, d));
+}
+
+// rebin_kernel's arithmetic with NQ 16-byte quads of rows per thread (4 NQ
+// rows sharing one (view, channel) index computation) and the blends in
+// packed pairs: half the instructions per sample, the same bits.
+template <int NQ>
+__global__ void __launch_bounds__(256) rebin_pk_kernel(float* __restrict__ out, const float* __restrict__ proj,
+                                                       const ChanInfo* __restrict__ chan, int YL, int ZL, int ViewN,
+                                                       float DeltaTheta, float DeltaFai) {
+  const int nkq = ZL / (4 * NQ);
+  const int jk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jk >= YL * nkq) return;
+  const int j = jk / nkq;
+  const int k = (jk - j * nkq) * 4 * NQ;
+  const ChanInfo c = chan[j];
+  const int YB = c.ybyu & 0xffff, YU = c.ybyu >> 16;
+  const size_t zl = (size_t)ZL;
+  for (int i = blockIdx.y; i < ViewN; i += gridDim.y) {
+    const float Theta = __fmul_rn((float)i, DeltaTheta);
+    const float Fai = __fadd_rn(Theta, c.beta);
+    const float FaiIndex = __fdiv_rn(Fai, DeltaFai);
+    const int FI = (int)ceilf(FaiIndex);
+    const float cxb = __fsub_rn((float)FI, FaiIndex);
+    const float cxu = __double2float_rn(__dsub_rn(1.0, (double)cxb));
+    int XU, XB;
+    if (FI <= 0) {
+      XU = 0;
+      XB = 0;
+    } else if (FI > ViewN - 1) {
+      XU = ViewN - 1;
+      XB = ViewN - 1;
+    } else {
+      XU = FI;
+      XB = FI - 1;
+    }
+    const float wbb = __fmul_rn(cxb, c.cyb), wub = __fmul_rn(cxu, c.cyb);
+    const float wbu = __fmul_rn(cxb, c.cyu), wuu = __fmul_rn(cxu, c.cyu);
+    const unsigned long long wbb2 = pack2(wbb, wbb), wub2 = pack2(wub, wub);
+    const unsigned long long wbu2 = pack2(wbu, wbu), wuu2 = pack2(wuu, wuu);
+    const ulonglong2* pa = reinterpret_cast<const ulonglong2*>(proj + ((size_t)XB * YL + YB) * zl + k);
+    const ulonglong2* pb = reinterpret_cast<const ulonglong2*>(proj + ((size_t)XU * YL + YB) * zl + k);
+    const ulonglong2* pc = reinterpret_cast<const ulonglong2*>(proj + ((size_t)XB * YL + YU) * zl + k);
+    const ulonglong2* pd = reinterpret_cast<const ulonglong2*>(proj + ((size_t)XU * YL + YU) * zl + k);
+    ulonglong2 a[NQ], b[NQ], cc[NQ], d[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      a[q] = pa[q];
+      b[q] = pb[q];
+      cc[q] = pc[q];
+      d[q] = pd[q];
+    }
+    ulonglong2* po = reinterpret_cast<ulonglong2*>(out + ((size_t)i * YL + j) * zl + k);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      ulonglong2 r;
+      r.x = blend2(wbb2, wub2, wbu2, wuu2, a[q].x, b[q].x, cc[q].x, d[q].x);
+      r.y = blend2(wbb2, wub2, wbu2, wuu2, a[q].y, b[q].y, cc[q].y, d[q].y);
+      po[q] = r;
+    }
+  }
+}
+
 // Per-channel values in the reference CPU's arithmetic
 // (ParallelRebinningCBCurve.cpp:37-48, 71-85 with T = float).
 void channel_table(std::vector<ChanInfo>& tab, int YL, float YLC, float dYA, float PLC, float DeltaT, float SO) {
@@ -166,22 +255,33 @@ extern "C" int hr_rebin_plan_create(hr_rebin_plan** plan, int YL, int ZL, int Vi
   return HR_OK;
 }
 
-extern "C" int hr_rebin_execute(const hr_rebin_plan* p, float* d_out, const float* d_proj, void* stream) {
+int hr::rebin_execute_limited(const hr_rebin_plan* p, float* d_out, const float* d_proj, int max_ctas,
+                              cudaStream_t s) {
   HR_REQUIRE(p != nullptr && d_out != nullptr && d_proj != nullptr, "hr_rebin_execute: NULL argument");
   HR_REQUIRE(d_out != d_proj, "hr_rebin_execute: in-place rebinning is not supported");
-  const bool vec4 = (p->ZL % 4 == 0) && ((uintptr_t)d_out % 16 == 0) && ((uintptr_t)d_proj % 16 == 0);
-  const int nkq = vec4 ? p->ZL / 4 : p->ZL;
+  const bool al16 = ((uintptr_t)d_out % 16 == 0) && ((uintptr_t)d_proj % 16 == 0);
+  const int nq = !al16 ? 0 : p->ZL % 8 == 0 ? 2 : p->ZL % 4 == 0 ? 1 : 0;  // 16-byte quads per thread
+  const int nkq = nq ? p->ZL / (4 * nq) : p->ZL;
   const int threads = 256;
-  dim3 grid((p->YL * nkq + threads - 1) / threads, p->ViewN < 65535 ? p->ViewN : 65535);
-  cudaStream_t s = hr::as_stream(stream);
-  if (vec4)
-    rebin_kernel<4><<<grid, threads, 0, s>>>(d_out, d_proj, p->d_chan, p->YL, p->ZL, p->ViewN, p->DeltaTheta,
-                                            p->DeltaFai);
+  const int gx = (p->YL * nkq + threads - 1) / threads;
+  int gy = p->ViewN < 65535 ? p->ViewN : 65535;  // the kernels stride over the views
+  if (max_ctas > 0) gy = std::max(1, std::min(gy, max_ctas / gx));
+  const dim3 grid(gx, gy);
+  if (nq == 2)
+    rebin_pk_kernel<2><<<grid, threads, 0, s>>>(d_out, d_proj, p->d_chan, p->YL, p->ZL, p->ViewN, p->DeltaTheta,
+                                               p->DeltaFai);
+  else if (nq == 1)
+    rebin_pk_kernel<1><<<grid, threads, 0, s>>>(d_out, d_proj, p->d_chan, p->YL, p->ZL, p->ViewN, p->DeltaTheta,
+                                               p->DeltaFai);
   else
     rebin_kernel<1><<<grid, threads, 0, s>>>(d_out, d_proj, p->d_chan, p->YL, p->ZL, p->ViewN, p->DeltaTheta,
                                             p->DeltaFai);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
+}
+
+extern "C" int hr_rebin_execute(const hr_rebin_plan* p, float* d_out, const float* d_proj, void* stream) {
+  return hr::rebin_execute_limited(p, d_out, d_proj, 0, hr::as_stream(stream));
 }
 
 extern "C" void hr_rebin_plan_destroy(hr_rebin_plan* p) {
