@@ -46,7 +46,8 @@ def test_fast_and_plain_hu_rmse_vs_fp64_oracle(cuda, cfg):
     assert 0.8 * G.MU_WATER < wl < 1.05 * G.MU_WATER
     fan_h = fan.cpu().numpy()
     del fan
-    zis = [sc.ZN // 2] if cfg == "small" else [sc.ZN // 3, 2 * sc.ZN // 3]
+    # full: the first and last slices (windows clamped to the scan's views) and two inner ones
+    zis = [sc.ZN // 2] if cfg == "small" else [0, sc.ZN // 3, 2 * sc.ZN // 3, sc.ZN - 1]
     step = 1 if cfg == "small" else 2
     ref, vox = reference_slices(sc, fan_h, zis, xy_step=step)
     # the reference CPU path rebins the whole scan in FP32 (bit-identical to the GPU rebinning)
@@ -59,12 +60,14 @@ def test_fast_and_plain_hu_rmse_vs_fp64_oracle(cuda, cfg):
     hu_plain = hu_rmse(plain.ravel()[vox], ref, wl)
     e_path = rel_l2(plain.ravel()[vox], refpath)
     e_f64 = rel_l2(plain.ravel()[vox], ref)
+    n = vox.size // len(zis)
+    per_slice = [rel_l2(plain.ravel()[vox[i * n:(i + 1) * n]], refpath[i * n:(i + 1) * n]) for i in range(len(zis))]
     print(f"[{cfg}] HU RMSE vs FP64 oracle: fast {hu_fast:.4f}  plain {hu_plain:.5f}  "
-          f"(water level {wl:.6f}, {vox.size} voxels); plain rel L2 vs reference path {e_path:.3e}, "
-          f"vs FP64 oracle {e_f64:.3e}")
+          f"(water level {wl:.6f}, {vox.size} voxels); plain rel L2 vs reference path {e_path:.3e} "
+          f"(by slice {', '.join(f'z{z}: {e:.2e}' for z, e in zip(zis, per_slice))}), vs FP64 oracle {e_f64:.3e}")
     assert hu_plain < 0.05
     assert hu_fast < HU_BUDGET
-    assert e_path < 1e-5
+    assert e_path < 1e-5 and max(per_slice) < 1e-5
 
 
 def test_fast_backprojection_matches_plain_on_the_same_data(cuda):
