@@ -420,23 +420,43 @@ __global__ void tex_absmax_kernel(float* __restrict__ scale, const uint32_t* __r
   if ((threadIdx.x & 31) == 0 && m) atomicMax(reinterpret_cast<unsigned*>(scale + 1), m);
 }
 
-// BF16 pairs [views][ZL][YL] -> the layered arrays. FP16: scaled by 2^k with
-// the largest |value| below 2^15; scale[0] = 2^-k, which the backprojection
-// folds into its output. One CTA row at a time (rows = views x ZL).
-template <bool HALF>
+// BF16 pairs [views][ZL][YL] -> the layered arrays, rows [r0, r1) (rows =
+// views x ZL; one CTA row at a time). FP16 (MODE 0): scaled by 2^k with the
+// largest |value| in [2^14, 2^15); scale[0] = 2^-k, which the backprojection
+// folds into its output. Views filled range by range while the fan data is
+// still arriving (a streamed execution) cannot know the largest |value| of the
+// scan: the first range (MODE 1) puts its own largest |value| in [2^10, 2^11)
+// and keeps the factor in scale[2]; later ranges (MODE 2) reuse it, and
+// scale[3] = 1 records that the running largest |value| (scale[1]) no longer
+// fits below FP16's largest finite value, or that the first range was all
+// zeros, so that the caller refills the whole copy with MODE 0. Any power of
+// two that keeps the values in FP16's normal range gives the same samples up
+// to that power.
+constexpr int kStreamHeadroom = 4;  // binades between the first range's largest |value| and MODE 0's range
+template <bool HALF, int MODE>
 __global__ void tex_fill_kernel(float* __restrict__ scale, const unsigned long long* __restrict__ surfs,
-                                const uint32_t* __restrict__ fpb, long long rows, int ZL, int YL, int lsh) {
+                                const uint32_t* __restrict__ fpb, long long r0, long long r1, int ZL, int YL,
+                                int lsh) {
   float sc = 1.0f;
-  if constexpr (HALF) {
+  if constexpr (HALF && MODE == 2) {
+    sc = scale[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && !(scale[1] * sc < 65504.0f)) scale[3] = 1.0f;
+  } else if constexpr (HALF) {
     const int e = (int)(__float_as_uint(scale[1]) >> 23) - 127;  // max |value| < 2^(e+1)
-    const int k = min(max(127 + 14 - e, 1), 253);                  // biased exponent of 2^(14-e)
+    const int k = min(max(127 + 14 - (MODE == 1 ? kStreamHeadroom : 0) - e, 1), 253);  // biased exponent of the factor
     sc = __int_as_float(k << 23);
-    if (blockIdx.x == 0 && threadIdx.x == 0) scale[0] = __int_as_float((254 - k) << 23);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      scale[0] = __int_as_float((254 - k) << 23);
+      if (MODE == 1) {
+        scale[2] = sc;
+        scale[3] = scale[1] == 0.0f ? 1.0f : 0.0f;
+      }
+    }
   } else {
     if (blockIdx.x == 0 && threadIdx.x == 0) scale[0] = 1.0f;
   }
   const int lmask = (1 << lsh) - 1;
-  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+  for (long long r = r0 + blockIdx.x; r < r1; r += gridDim.x) {
     const int p = (int)(r / ZL), v = (int)(r - (long long)p * ZL);
     const cudaSurfaceObject_t so = surfs[p >> lsh];
     const uint32_t* row = fpb + r * YL;
@@ -963,6 +983,7 @@ int bp_fast_upload(BpFast* f, const BpFastHost& h, cudaStream_t s) {
                                 s));
     HR_CUDA_TRY(cudaMemcpyAsync(t.d_zblock, ht.zb.data(), sizeof(int) * ht.zb.size(), cudaMemcpyHostToDevice, s));
     HR_CUDA_TRY(cudaMemcpyAsync(t.d_seg, ht.seg.data(), sizeof(int4) * ht.seg.size(), cudaMemcpyHostToDevice, s));
+    t.h_zb.assign(ht.zb.begin(), ht.zb.begin() + 2 * (size_t)ht.nblocks);
   }
   HR_REQUIRE(h.trig.size() <= (size_t)f->cap_views, "fast backprojection: more views than reserved");
   HR_CUDA_TRY(cudaMemcpyAsync(f->d_trig, h.trig.data(), sizeof(float2) * h.trig.size(), cudaMemcpyHostToDevice, s));
@@ -1041,7 +1062,7 @@ static int tex_alloc_arrays(BpFastTex* t, int kind, int YL, int ZL, int views) {
   obj.insert(obj.end(), t->surf.begin(), t->surf.end());
   HR_CUDA_TRY(cudaMalloc(&t->d_obj, sizeof(unsigned long long) * obj.size()));
   HR_CUDA_TRY(cudaMemcpy(t->d_obj, obj.data(), sizeof(unsigned long long) * obj.size(), cudaMemcpyHostToDevice));
-  HR_CUDA_TRY(cudaMalloc(&t->d_scale, 2 * sizeof(float)));
+  HR_CUDA_TRY(cudaMalloc(&t->d_scale, 4 * sizeof(float)));
   t->bytes = (size_t)views * YL * ZL * esz;
   return HR_OK;
 }
@@ -1062,20 +1083,41 @@ int bp_fast_tex_prepare(BpFast* f, const BpFastGeom& g) {
 
 // BF16 pairs of the geometry's views -> the plan's layered arrays.
 int bp_fast_tex_fill(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, cudaStream_t s) {
+  return bp_fast_tex_fill_range(f, g, fpb, 0, g.PN, 0, s);
+}
+
+int bp_fast_tex_fill_range(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, int p0, int p1, int mode,
+                           cudaStream_t s) {
   const BpFastTex& t = f.tex;
   HR_REQUIRE(t.kind != 0 && t.views >= g.PN && t.YL == g.YL && t.ZL == g.ZL,
              "fast backprojection: the textures of variant %d are not prepared", f.variant);
-  const long long rows = (long long)g.PN * g.ZL;
-  const int grid = (int)std::min<long long>(rows, 16LL * sm_count());
-  if (rows == 0) return HR_OK;
+  HR_REQUIRE(0 <= p0 && p0 <= p1 && p1 <= g.PN && mode >= 0 && mode <= 2, "fast backprojection: fill of views "
+             "[%d, %d) (mode %d) outside [0, %d)", p0, p1, mode, g.PN);
+  const long long r0 = (long long)p0 * g.ZL, r1 = (long long)p1 * g.ZL;
+  const int grid = (int)std::max(1LL, std::min<long long>(r1 - r0, 16LL * sm_count()));
   if (t.kind == kTexHalf) {
-    HR_CUDA_TRY(cudaMemsetAsync(t.d_scale + 1, 0, sizeof(float), s));
-    tex_absmax_kernel<<<4 * sm_count(), 256, 0, s>>>(t.d_scale, fpb, rows * g.YL);
-    tex_fill_kernel<true><<<grid, 256, 0, s>>>(t.d_scale, t.d_obj + t.n, fpb, rows, g.ZL, g.YL, t.lsh);
+    if (mode != 2) HR_CUDA_TRY(cudaMemsetAsync(t.d_scale + 1, 0, sizeof(float), s));
+    if (r1 > r0) tex_absmax_kernel<<<4 * sm_count(), 256, 0, s>>>(t.d_scale, fpb + r0 * g.YL, (r1 - r0) * g.YL);
+    if (mode == 0)
+      tex_fill_kernel<true, 0><<<grid, 256, 0, s>>>(t.d_scale, t.d_obj + t.n, fpb, r0, r1, g.ZL, g.YL, t.lsh);
+    else if (mode == 1)
+      tex_fill_kernel<true, 1><<<grid, 256, 0, s>>>(t.d_scale, t.d_obj + t.n, fpb, r0, r1, g.ZL, g.YL, t.lsh);
+    else
+      tex_fill_kernel<true, 2><<<grid, 256, 0, s>>>(t.d_scale, t.d_obj + t.n, fpb, r0, r1, g.ZL, g.YL, t.lsh);
   } else {
-    tex_fill_kernel<false><<<grid, 256, 0, s>>>(t.d_scale, t.d_obj + t.n, fpb, rows, g.ZL, g.YL, t.lsh);
+    if (mode == 1) HR_CUDA_TRY(cudaMemsetAsync(t.d_scale + 3, 0, sizeof(float), s));
+    tex_fill_kernel<false, 0><<<grid, 256, 0, s>>>(t.d_scale, t.d_obj + t.n, fpb, r0, r1, g.ZL, g.YL, t.lsh);
   }
   HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
+int bp_fast_tex_refill_needed(const BpFast& f, bool* needed) {
+  *needed = false;
+  if (f.tex.kind != kTexHalf) return HR_OK;
+  float flag = 0.f;
+  HR_CUDA_TRY(cudaMemcpy(&flag, f.tex.d_scale + 3, sizeof(float), cudaMemcpyDeviceToHost));
+  *needed = flag != 0.f;
   return HR_OK;
 }
 
@@ -1345,6 +1387,16 @@ int bp_fast_execute(const BpFast& f, const BpFastGeom& g, float* vol, const uint
   if (kFastVariants[f.variant].tex) HR_TRY(bp_fast_tex_fill(f, g, fpb, s));
   return run_variant(f, g, f.variant, vol, fpb, 0, -1, s);
 }
+
+int bp_fast_execute_blocks(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, int b_first,
+                           int b_count, cudaStream_t s) {
+  const BpFastTables& t = f.t[kFastVariants[f.variant].table];
+  HR_REQUIRE(b_first >= 0 && b_count >= 0 && b_first + b_count <= t.nblocks,
+             "fast backprojection: z blocks [%d, %d) outside [0, %d)", b_first, b_first + b_count, t.nblocks);
+  return run_variant(f, g, f.variant, vol, fpb, b_first, b_count, s);
+}
+
+const BpFastTables& bp_fast_variant_tables(const BpFast& f) { return f.t[kFastVariants[f.variant].table]; }
 
 // HELIXRECON_BP_VARIANT=<index> pins the variant and skips the timing (for
 // profiling runs, whose serialised launches would skew the choice, and for

@@ -64,6 +64,7 @@ struct BpFastTables {
   int* d_zblock = nullptr;     // [nblocks] {first view, count}, then [nblocks] table offsets
   int4* d_seg = nullptr;       // [nblocks][kSegPerNz NZ] view segments
   size_t bytes = 0;
+  std::vector<int> h_zb;       // host copy of the [nblocks] {first view, count} of the last upload
 };
 
 // Host copies of one geometry's tables (built in FP64, uploaded as float).
@@ -124,6 +125,21 @@ int bp_fast_describe(const BpFast& f, char* buf, int len);
 int bp_fast_tex_prepare(BpFast* f, const BpFastGeom& g);
 // Fills the plan's layered textures from BF16 pairs (stream-ordered).
 int bp_fast_tex_fill(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, cudaStream_t s);
+// Fills views [p0, p1) only. mode 0: the FP16 scale from these views' largest |value| (a whole fill); 1: the
+// first range of a fill done range by range while later views are still being produced (its scale leaves
+// headroom for larger values later); 2: a later range with the first range's scale. After a fill by ranges,
+// bp_fast_tex_refill_needed (synchronous) says whether a later range's values exceeded the FP16 range of that
+// scale (or the first range was all zeros); the copy must then be refilled whole (mode 0) before its samples
+// are used again.
+int bp_fast_tex_fill_range(const BpFast& f, const BpFastGeom& g, const uint32_t* fpb, int p0, int p1, int mode,
+                           cudaStream_t s);
+int bp_fast_tex_refill_needed(const BpFast& f, bool* needed);
+// Backprojects z blocks [b_first, b_first + b_count) of the plan's variant (a texture variant samples the
+// copy as it is: no fill).
+int bp_fast_execute_blocks(const BpFast& f, const BpFastGeom& g, float* vol, const uint32_t* fpb, int b_first,
+                           int b_count, cudaStream_t s);
+// The z-block tables of the plan's variant (nz slices per block; h_zb: each block's view window).
+const BpFastTables& bp_fast_variant_tables(const BpFast& f);
 // Several scans in one persistent launch. Each scan runs the kernel body with
 // its own slices per thread (16, 8 or 4; 8 or 4 with texture taps); batch
 // variants differ in the CTAs (of 256 threads) per SM their registers must

@@ -497,6 +497,10 @@ int hr::filter_tc_create_shared(hr_filter_tc_plan** plan, int YL, int ZL, int Vi
   return tc_create(plan, YL, ZL, ViewN, PLC, ZLC, dYL, dZL, SO, scratch);
 }
 
+void hr::filter_tc_scratch(const hr_filter_tc_plan* p, void* scratch[3]) {
+  for (int i = 0; i < kParts; ++i) scratch[i] = p->d_a[i];
+}
+
 extern "C" int hr_filter_tc_plan_create(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float PLC, float ZLC,
                                         float dYL, float dZL, float SO) {
   hr::clear_error();

@@ -79,6 +79,14 @@ int filter_tc_create_shared(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN,
 // the public entries): memory-bound stages that run beside a texture-bound
 // backprojection leave it most of the SMs' CTA slots.
 int rebin_execute_limited(const hr_rebin_plan* p, float* d_out, const float* d_proj, int max_ctas, cudaStream_t s);
+// Output views [i0, i1) only (written at their place in d_out; the same bits as a whole-scan launch).
+int rebin_execute_range(const hr_rebin_plan* p, float* d_out, const float* d_proj, int i0, int i1, int max_ctas,
+                        cudaStream_t s);
+// Fan views [*f0, *f1] (clamped to the scan) that output views [i0, i1) read; i0 < i1.
+void rebin_fan_views(const hr_rebin_plan* p, int i0, int i1, int* f0, int* f1);
+// The three split-operand buffers of a tensor-core filter plan (its own or a caller's scratch), for plans that
+// share them with filter_tc_create_shared.
+void filter_tc_scratch(const hr_filter_tc_plan* p, void* scratch[3]);
 int filter_tc_execute_limited(const hr_filter_tc_plan* p, uint32_t* d_pairs, const float* d_in, int in_layout,
                               int view0, int max_prep_ctas, cudaStream_t s);
 

@@ -21,7 +21,9 @@
 // Layout [ViewN][YL][ZL], ZL fastest: the ZL rows of one (view, channel) are
 // contiguous, so a thread moves 4 rows at once (16-byte loads/stores) and the
 // four taps of a warp are contiguous runs. Grid: x over (channel, row quad),
-// y over views (grid-stride beyond 65535).
+// y over the output views [i0, i1) (grid-stride beyond 65535); the clamp is
+// always against the whole scan's ViewN, so a range of views has the bits of
+// the same views of a whole-scan launch.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -39,6 +41,7 @@ struct hr_rebin_plan {
   int YL, ZL, ViewN;
   float DeltaTheta, DeltaFai;
   ChanInfo* d_chan;
+  float beta_lo, beta_hi;  // smallest and largest per-channel angle offset (for hr::rebin_fan_views)
 };
 
 namespace {
@@ -66,7 +69,7 @@ __device__ __forceinline__ float blend4(float wbb, float wub, float wbu, float w
 template <int VEC>
 __global__ void __launch_bounds__(256) rebin_kernel(float* __restrict__ out, const float* __restrict__ proj,
                                                     const ChanInfo* __restrict__ chan, int YL, int ZL, int ViewN,
-                                                    float DeltaTheta, float DeltaFai) {
+                                                    float DeltaTheta, float DeltaFai, int i0, int i1) {
   using V = typename VecT<VEC>::T;
   const int nkq = ZL / VEC;
   const int jk = blockIdx.x * blockDim.x + threadIdx.x;
@@ -75,7 +78,7 @@ __global__ void __launch_bounds__(256) rebin_kernel(float* __restrict__ out, con
   const int k = (jk - j * nkq) * VEC;
   const ChanInfo c = chan[j];
   const int YB = c.ybyu & 0xffff, YU = c.ybyu >> 16;
-  for (int i = blockIdx.y; i < ViewN; i += gridDim.y) {
+  for (int i = i0 + (int)blockIdx.y; i < i1; i += gridDim.y) {
     const float Theta = __fmul_rn((float)i, DeltaTheta);
     const float Fai = __fadd_rn(Theta, c.beta);
     const float FaiIndex = __fdiv_rn(Fai, DeltaFai);
@@ -113,41 +116,16 @@ __global__ void __launch_bounds__(256) rebin_kernel(float* __restrict__ out, con
   }
 }
 
-// Packed FP32x2 arithmetic (one instruction for two lanes; each lane rounded
-// to nearest like the scalar mul.rn / add.rn, no contraction).
-__device__ __forceinline__ unsigned long long pack2(float a, float b) {
-  unsigned long long r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-  return r;
-}
-__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
-  unsigned long long d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
-  unsigned long long d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-// blend4 on a pair of rows.
-__device__ __forceinline__ unsigned long long blend2(unsigned long long wbb, unsigned long long wub,
-                                                     unsigned long long wbu, unsigned long long wuu,
-                                                     unsigned long long a, unsigned long long b,
-                                                     unsigned long long c, unsigned long long d) {
-  unsigned long long acc = mul2(wbb, a);
-  acc = add2(acc, mul2(wub, b));
-  acc = add2(acc, mul2(wbu, c));
-  return add2(acc, mul2(wuu, d));
-}
-
-// rebin_kernel's arithmetic with NQ 16-byte quads of rows per thread (4 NQ
-// rows sharing one (view, channel) index computation) and the blends in
-// packed pairs: half the instructions per sample, the same bits.
+// rebin_kernel's arithmetic with NQ 16-byte quads of rows per thread: 4 NQ
+// rows share one (view, channel) index computation, and every row is blended
+// with the same scalar non-contracting operations, so the bits are the same.
+// (Packed FP32x2 multiplies and adds were tried for the blends and measured
+// 1-2 ulp away from the reference on a quarter of the samples: they do not
+// round like the scalar mul.rn / add.rn sequence.)
 template <int NQ>
-__global__ void __launch_bounds__(256) rebin_pk_kernel(float* __restrict__ out, const float* __restrict__ proj,
+__global__ void __launch_bounds__(256) rebin_rows_kernel(float* __restrict__ out, const float* __restrict__ proj,
                                                        const ChanInfo* __restrict__ chan, int YL, int ZL, int ViewN,
-                                                       float DeltaTheta, float DeltaFai) {
+                                                       float DeltaTheta, float DeltaFai, int i0, int i1) {
   const int nkq = ZL / (4 * NQ);
   const int jk = blockIdx.x * blockDim.x + threadIdx.x;
   if (jk >= YL * nkq) return;
@@ -156,7 +134,7 @@ __global__ void __launch_bounds__(256) rebin_pk_kernel(float* __restrict__ out, 
   const ChanInfo c = chan[j];
   const int YB = c.ybyu & 0xffff, YU = c.ybyu >> 16;
   const size_t zl = (size_t)ZL;
-  for (int i = blockIdx.y; i < ViewN; i += gridDim.y) {
+  for (int i = i0 + (int)blockIdx.y; i < i1; i += gridDim.y) {
     const float Theta = __fmul_rn((float)i, DeltaTheta);
     const float Fai = __fadd_rn(Theta, c.beta);
     const float FaiIndex = __fdiv_rn(Fai, DeltaFai);
@@ -176,13 +154,11 @@ __global__ void __launch_bounds__(256) rebin_pk_kernel(float* __restrict__ out, 
     }
     const float wbb = __fmul_rn(cxb, c.cyb), wub = __fmul_rn(cxu, c.cyb);
     const float wbu = __fmul_rn(cxb, c.cyu), wuu = __fmul_rn(cxu, c.cyu);
-    const unsigned long long wbb2 = pack2(wbb, wbb), wub2 = pack2(wub, wub);
-    const unsigned long long wbu2 = pack2(wbu, wbu), wuu2 = pack2(wuu, wuu);
-    const ulonglong2* pa = reinterpret_cast<const ulonglong2*>(proj + ((size_t)XB * YL + YB) * zl + k);
-    const ulonglong2* pb = reinterpret_cast<const ulonglong2*>(proj + ((size_t)XU * YL + YB) * zl + k);
-    const ulonglong2* pc = reinterpret_cast<const ulonglong2*>(proj + ((size_t)XB * YL + YU) * zl + k);
-    const ulonglong2* pd = reinterpret_cast<const ulonglong2*>(proj + ((size_t)XU * YL + YU) * zl + k);
-    ulonglong2 a[NQ], b[NQ], cc[NQ], d[NQ];
+    const float4* pa = reinterpret_cast<const float4*>(proj + ((size_t)XB * YL + YB) * zl + k);
+    const float4* pb = reinterpret_cast<const float4*>(proj + ((size_t)XU * YL + YB) * zl + k);
+    const float4* pc = reinterpret_cast<const float4*>(proj + ((size_t)XB * YL + YU) * zl + k);
+    const float4* pd = reinterpret_cast<const float4*>(proj + ((size_t)XU * YL + YU) * zl + k);
+    float4 a[NQ], b[NQ], cc[NQ], d[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
       a[q] = pa[q];
@@ -190,12 +166,14 @@ __global__ void __launch_bounds__(256) rebin_pk_kernel(float* __restrict__ out, 
       cc[q] = pc[q];
       d[q] = pd[q];
     }
-    ulonglong2* po = reinterpret_cast<ulonglong2*>(out + ((size_t)i * YL + j) * zl + k);
+    float4* po = reinterpret_cast<float4*>(out + ((size_t)i * YL + j) * zl + k);
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
-      ulonglong2 r;
-      r.x = blend2(wbb2, wub2, wbu2, wuu2, a[q].x, b[q].x, cc[q].x, d[q].x);
-      r.y = blend2(wbb2, wub2, wbu2, wuu2, a[q].y, b[q].y, cc[q].y, d[q].y);
+      float4 r;
+      r.x = blend4(wbb, wub, wbu, wuu, a[q].x, b[q].x, cc[q].x, d[q].x);
+      r.y = blend4(wbb, wub, wbu, wuu, a[q].y, b[q].y, cc[q].y, d[q].y);
+      r.z = blend4(wbb, wub, wbu, wuu, a[q].z, b[q].z, cc[q].z, d[q].z);
+      r.w = blend4(wbb, wub, wbu, wuu, a[q].w, b[q].w, cc[q].w, d[q].w);
       po[q] = r;
     }
   }
@@ -242,7 +220,11 @@ extern "C" int hr_rebin_plan_create(hr_rebin_plan** plan, int YL, int ZL, int Vi
   HR_TRY(hr::require_device());
   std::vector<ChanInfo> tab;
   channel_table(tab, YL, YLC, dYA, PLC, DeltaT, SO);
-  hr_rebin_plan* p = new hr_rebin_plan{YL, ZL, ViewN, DeltaTheta, DeltaFai, nullptr};
+  hr_rebin_plan* p = new hr_rebin_plan{YL, ZL, ViewN, DeltaTheta, DeltaFai, nullptr, tab[0].beta, tab[0].beta};
+  for (const ChanInfo& c : tab) {
+    p->beta_lo = std::min(p->beta_lo, c.beta);
+    p->beta_hi = std::max(p->beta_hi, c.beta);
+  }
   cudaError_t e = cudaMalloc(&p->d_chan, sizeof(ChanInfo) * YL);
   if (e == cudaSuccess) e = cudaMemcpy(p->d_chan, tab.data(), sizeof(ChanInfo) * YL, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -255,29 +237,55 @@ extern "C" int hr_rebin_plan_create(hr_rebin_plan** plan, int YL, int ZL, int Vi
   return HR_OK;
 }
 
-int hr::rebin_execute_limited(const hr_rebin_plan* p, float* d_out, const float* d_proj, int max_ctas,
-                              cudaStream_t s) {
+int hr::rebin_execute_range(const hr_rebin_plan* p, float* d_out, const float* d_proj, int i0, int i1, int max_ctas,
+                            cudaStream_t s) {
   HR_REQUIRE(p != nullptr && d_out != nullptr && d_proj != nullptr, "hr_rebin_execute: NULL argument");
   HR_REQUIRE(d_out != d_proj, "hr_rebin_execute: in-place rebinning is not supported");
+  HR_REQUIRE(0 <= i0 && i0 <= i1 && i1 <= p->ViewN, "hr_rebin_execute: views [%d, %d) outside [0, %d)", i0, i1,
+             p->ViewN);
+  if (i1 == i0) return HR_OK;
   const bool al16 = ((uintptr_t)d_out % 16 == 0) && ((uintptr_t)d_proj % 16 == 0);
   const int nq = !al16 ? 0 : p->ZL % 8 == 0 ? 2 : p->ZL % 4 == 0 ? 1 : 0;  // 16-byte quads per thread
   const int nkq = nq ? p->ZL / (4 * nq) : p->ZL;
   const int threads = 256;
   const int gx = (p->YL * nkq + threads - 1) / threads;
-  int gy = p->ViewN < 65535 ? p->ViewN : 65535;  // the kernels stride over the views
+  int gy = std::min(i1 - i0, 65535);  // the kernels stride over the views
   if (max_ctas > 0) gy = std::max(1, std::min(gy, max_ctas / gx));
   const dim3 grid(gx, gy);
   if (nq == 2)
-    rebin_pk_kernel<2><<<grid, threads, 0, s>>>(d_out, d_proj, p->d_chan, p->YL, p->ZL, p->ViewN, p->DeltaTheta,
-                                               p->DeltaFai);
+    rebin_rows_kernel<2><<<grid, threads, 0, s>>>(d_out, d_proj, p->d_chan, p->YL, p->ZL, p->ViewN, p->DeltaTheta,
+                                               p->DeltaFai, i0, i1);
   else if (nq == 1)
-    rebin_pk_kernel<1><<<grid, threads, 0, s>>>(d_out, d_proj, p->d_chan, p->YL, p->ZL, p->ViewN, p->DeltaTheta,
-                                               p->DeltaFai);
+    rebin_rows_kernel<1><<<grid, threads, 0, s>>>(d_out, d_proj, p->d_chan, p->YL, p->ZL, p->ViewN, p->DeltaTheta,
+                                               p->DeltaFai, i0, i1);
   else
     rebin_kernel<1><<<grid, threads, 0, s>>>(d_out, d_proj, p->d_chan, p->YL, p->ZL, p->ViewN, p->DeltaTheta,
-                                            p->DeltaFai);
+                                            p->DeltaFai, i0, i1);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
+}
+
+int hr::rebin_execute_limited(const hr_rebin_plan* p, float* d_out, const float* d_proj, int max_ctas,
+                              cudaStream_t s) {
+  HR_REQUIRE(p != nullptr, "hr_rebin_execute: NULL argument");
+  return rebin_execute_range(p, d_out, d_proj, 0, p->ViewN, max_ctas, s);
+}
+
+// Output view i reads the fan views FI - 1 and FI with FI = ceil((i DeltaTheta + beta_j) / DeltaFai) over the
+// channels j (clamped to the scan). Bounded here in double with one view of slack on each side for the float
+// rounding of the kernel's arithmetic.
+void hr::rebin_fan_views(const hr_rebin_plan* p, int i0, int i1, int* f0, int* f1) {
+  const double dt = p->DeltaTheta, df = p->DeltaFai;
+  double a = 1e300, b = -1e300;  // FaiIndex is monotone in i and in beta: its extremes are at the corners
+  for (const int i : {i0, i1 - 1})
+    for (const float beta : {p->beta_lo, p->beta_hi}) {
+      const double x = (i * dt + beta) / df;
+      a = std::min(a, x);
+      b = std::max(b, x);
+    }
+  const double lo = std::floor(a) - 2.0, hi = std::ceil(b) + 1.0;
+  *f0 = (int)std::max(0.0, std::min(lo, (double)(p->ViewN - 1)));
+  *f1 = (int)std::max(0.0, std::min(hi, (double)(p->ViewN - 1)));
 }
 
 extern "C" int hr_rebin_execute(const hr_rebin_plan* p, float* d_out, const float* d_proj, void* stream) {

@@ -380,7 +380,9 @@ def measure_form(args, scan, form, fan, dev, world, barrier, with_e2e=True):
         e2e_s = statistics.median(e2e_t)
         (e2e_s,) = max_over_ranks([e2e_s], world, dev)
         out["e2e_s"] = e2e_s
-        out["e2e_entry"] = "hr_recon_execute_host (C ABI, pinned host buffers)"
+        out["e2e_entry"] = ("hr_recon_execute_host (C ABI, pinned host buffers; the fan streams in by chunks of "
+                            "views under the rebinning, filtering and z-block backprojection of the earlier ones)"
+                            if fast else "hr_recon_execute_host (C ABI, pinned host buffers)")
         slab_sizes = [int(x) for x in str(args.e2e_slab).split(",") if x.strip() and int(x) > 0]
         if fast and slab_sizes:
             # the same volume through the slab pipeline: host-to-device copies of later slabs' fan windows

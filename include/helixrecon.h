@@ -260,7 +260,16 @@ int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* desc);
 /* Device pointers: d_fan [ViewN][YL][ZL] float, d_vol [YN][XN][ZN] float. */
 int hr_recon_execute(const hr_recon_plan* plan, float* d_vol, const float* d_fan, void* stream);
 /* Host pointers (pinned for full copy speed): copies the fan data in, runs the
- * chain, copies the volume out; returns when h_vol is written. */
+ * chain, copies the volume out; returns when h_vol is written. The fast form
+ * streams: the fan crosses the host link in chunks of 1024 views
+ * (HELIXRECON_STREAM_CHUNK at plan creation; 0: no streaming) while the chunks
+ * that have arrived are rebinned and filtered, z-block ranges are
+ * backprojected as soon as their view windows are filtered, and each range's
+ * slices are copied out while later ranges compute. Rebinning and filtering
+ * give the device entry's bits; a texture variant's FP16 copy is filled chunk
+ * by chunk with a scale from the first chunk (2^4 of headroom), so its volume
+ * equals the device entry's to FP32 rounding, and is refilled whole (the
+ * device entry's bits) when a later chunk exceeds that scale. */
 int hr_recon_execute_host(hr_recon_plan* plan, float* h_vol, const float* h_fan);
 /* One-line description of the plan's kernel configuration (the fast form's
  * backprojection is autotuned at plan creation). */
