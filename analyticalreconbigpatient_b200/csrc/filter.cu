@@ -34,6 +34,7 @@
 // straight to the output rows. Two shared-memory exchanges per pair of rows,
 // no block-wide barrier after set-up.
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "hr_internal.h"
@@ -45,6 +46,10 @@ struct hr_filter_plan {
   float2* d_tw;  // exp(-2 pi i t / N), t in [0, N)
   float* d_wt;   // N = 2048: preweight of every (row k, channel j), [ZL][YL]
   float2* d_tw2; // N = 2048: W_2048^(j c) as [c][j], c in [0, 64), j in [0, 32)
+  float2* d_tw3; // N = 2048, two warps per row pair: W_2048^(j k1) as [k1][j], k1 in [0, 32), j in [0, 64)
+  float2* d_G;   // N = 2048, two warps per row pair: {H[k1 + 32 k] + H[k1 + 32 k + 1024], difference} at [k][k1]
+  float* d_wt8;  // N = 2048, ZL % 8 == 0: d_wt as [ZL / 8][YL][8] (the staged rebinning-layout path)
+  int kernel2048;  // 0: two warps per row pair; 1: one warp per row pair (HELIXRECON_FILTER2048=1)
 };
 
 namespace {
@@ -329,15 +334,18 @@ __device__ __forceinline__ void dft32_inv(float2 (&v)[32]) {
 __device__ __forceinline__ int dft32_freq(int p) { return (p >> 2) + 8 * (p & 3); }
 
 // Preweight table [ZL][YL] with the reference's float expression
-// (src/filtering.cu:187-207).
-__global__ void preweight_table_kernel(float* __restrict__ wt, int YL, int ZL, float PLC, float ZLC, float dYL,
-                                       float dZL, float SO) {
+// (src/filtering.cu:187-207); wt8 (if not null): the same values as
+// [ZL / 8][YL][8].
+__global__ void preweight_table_kernel(float* __restrict__ wt, float* __restrict__ wt8, int YL, int ZL, float PLC,
+                                       float ZLC, float dYL, float dZL, float SO) {
   const float SO2 = SO * SO;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < YL * ZL; e += gridDim.x * blockDim.x) {
     const int k = e / YL, j = e - k * YL;
     const float b = ((float)k - ZLC) * dZL;
     const float t = ((float)j - PLC) * dYL;
-    wt[e] = SO2 / sqrtf(SO2 * (SO2 + b * b) - b * t * b * t);
+    const float w = SO2 / sqrtf(SO2 * (SO2 + b * b) - b * t * b * t);
+    wt[e] = w;
+    if (wt8) wt8[((size_t)(k >> 3) * YL + j) * 8 + (k & 7)] = w;
   }
 }
 
@@ -517,6 +525,196 @@ int launch(const hr_filter_plan* p, float* out, const float* in, int view0, cuda
   return launch_k<IN_LAYOUT, false>(p, out, in, view0, s);
 }
 
+// ---- two warps per row pair ------------------------------------------------
+// N = 64 x 32 with 32 points per lane, so that a lane needs half the registers
+// of the one-warp kernel (<= 128: 16 warps per SM instead of 8). The 64 lanes
+// of a pair (j = lane + 32 h, h the warp of the pair) and x[n], n = j + 64 m:
+//   A: lane j: 32-point DFT over m -> k1, times W_2048^(j k1), into row j of
+//      the pair's exchange buffer [64][33].
+//   B: column k1 (lane & 15 + 16 h) is shared by lanes l and l ^ 16 (e =
+//      lane >> 4): lane e takes rows j = 2 j' + e and transforms over j' -> k
+//      (E for e = 0, O for e = 1). The 64-point DFT over j is X[k1 + 32 k] =
+//      E + W_64^k O and X[k1 + 32 (k + 32)] = E - W_64^k O; after the filter
+//      (H0 = H[k1 + 32 k], H1 = H[k1 + 32 k + 1024]) the inverse over k2 needs
+//      S = Y0 + Y1 = (H0 + H1) E + (H0 - H1) W_64^k O on the even rows and
+//      D = W_64^-k (Y0 - Y1) = (H0 - H1) W_64^-k E + (H0 + H1) O on the odd
+//      ones, so one exchange of E and O between the two lanes (a shuffle)
+//      carries the forward radix-2 step, the filter and the inverse one. An
+//      inverse 32-point DFT over k gives rows 2 j' + e, times
+//      conj(W_2048^(j k1)), back into the buffer.
+//   A': lane j: inverse 32-point DFT over k1 of row j -> y[j + 64 m].
+// With YL <= 64 MNZ only m < MNZ carries samples (888 channels: 14 of 32), so
+// the first forward stage and the last inverse one are pruned at compile time.
+// Bank-conflict free: rows of 33 float2 for the row-wise stages, 16
+// consecutive columns per half-warp for the column-wise one.
+constexpr int kPairs = 4;             // row pairs per CTA, two warps each
+constexpr int kThreads2 = 64 * kPairs;
+constexpr int kS2 = 33;               // exchange row stride in float2
+
+__device__ __forceinline__ void bar_pair(int pair) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + pair), "r"(64) : "memory");
+}
+
+template <int IN_LAYOUT, bool STAGE, int MNZ>
+__global__ void __launch_bounds__(kThreads2, 2) filter2048x2_kernel(float* __restrict__ out,
+                                                                   const float* __restrict__ in,
+                                                                   const float2* __restrict__ gtw,
+                                                                   const float2* __restrict__ gG,
+                                                                   const float* __restrict__ wt, int YL, int ZL,
+                                                                   long long rows, int view0) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* twA = reinterpret_cast<float2*>(smem_raw);  // [32][64]: W_2048^(j k1) at [k1][j]
+  float2* twB = twA + 32 * 64;                        // [64][32]: the same at [j][k1]
+  float2* G = twB + 64 * 32;                          // [32][32]: {H0 + H1, H0 - H1} at [k][k1]
+  float2* xall = G + 32 * 32;                         // kPairs exchange buffers [64][kS2]
+  for (int t = threadIdx.x; t < 32 * 64; t += kThreads2) {
+    const float2 w = gtw[t];
+    twA[t] = w;
+    twB[(t & 63) * 32 + (t >> 6)] = w;
+  }
+  for (int t = threadIdx.x; t < 32 * 32; t += kThreads2) G[t] = gG[t];
+  __syncthreads();
+  const int pair = threadIdx.x >> 6, h = (threadIdx.x >> 5) & 1, lane = threadIdx.x & 31;
+  const int j = lane + 32 * h;                      // stages A and A'
+  const int kc = (lane & 15) + 16 * h, e = lane >> 4;  // stage B: column and row parity
+  float2* xb = xall + pair * 64 * kS2;
+  float* stage = reinterpret_cast<float*>(xall);    // [YL][10] (STAGE), over the exchange buffers
+  const long long npairs = (rows + 1) >> 1;
+  // STAGE: rows is a multiple of 8, so every tile of kPairs pairs is full and the loop is CTA-uniform
+  const long long first = STAGE ? (long long)blockIdx.x * kPairs : (long long)blockIdx.x * kPairs + pair;
+  const long long step = (long long)gridDim.x * kPairs;
+  for (long long pt = first; pt < npairs; pt += step) {
+    const long long pr = STAGE ? pt + pair : pt;
+    const long long ra = 2 * pr, rb = ra + 1;
+    const bool hasb = rb < rows;
+    float2 v[32];
+    if constexpr (STAGE) {
+      // rows 2 pt .. 2 pt + 7 are k0 .. k0 + 7 of one view (ZL % 8 == 0): stage them preweighted
+      const long long r0 = 2 * pt;
+      const long long va0 = r0 / ZL;
+      const int k0 = (int)(r0 - va0 * ZL);
+      const float4* src = reinterpret_cast<const float4*>(in + (size_t)(view0 + va0) * YL * ZL + k0);
+      __syncthreads();  // every pair has finished reading its exchange buffer (the previous tile)
+      // wt here: the preweights as [ZL / 8][YL][8], the 8 rows of a channel in 32 contiguous bytes
+      const float4* w8 = reinterpret_cast<const float4*>(wt + ((size_t)(k0 >> 3) * YL) * 8);
+      for (int t = threadIdx.x; t < 2 * YL; t += kThreads2) {
+        const int n = t >> 1, hq = t & 1;
+        const float4 q = __ldg(src + (size_t)n * (ZL / 4) + hq);
+        const float4 w = __ldg(w8 + 2 * n + hq);
+        float2* d = reinterpret_cast<float2*>(stage + n * 10 + 4 * hq);
+        d[0] = make_float2(q.x * w.x, q.y * w.y);
+        d[1] = make_float2(q.z * w.z, q.w * w.w);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < 32; ++m) {
+        const int n = j + 64 * m;
+        v[m] = make_float2(0.f, 0.f);
+        if (m < MNZ && n < YL) v[m] = *reinterpret_cast<const float2*>(stage + n * 10 + 2 * pair);
+      }
+      __syncthreads();  // the staging area is read before any pair writes its exchange buffer
+    } else {
+      bar_pair(pair);  // both warps of the pair have finished reading the buffer (the previous pair of rows)
+      const int ka = (int)(ra % ZL), kb = (int)(rb % ZL);
+      const long long va = ra / ZL, vb = rb / ZL;
+      const float* pa = IN_LAYOUT == HR_LAYOUT_ROWS ? in + ((size_t)(view0 + va) * ZL + ka) * YL
+                                                    : in + (size_t)(view0 + va) * YL * ZL + ka;
+      const float* pb = IN_LAYOUT == HR_LAYOUT_ROWS ? in + ((size_t)(view0 + vb) * ZL + kb) * YL
+                                                    : in + (size_t)(view0 + vb) * YL * ZL + kb;
+      const size_t es = IN_LAYOUT == HR_LAYOUT_ROWS ? 1 : (size_t)ZL;  // element stride along a row
+      const float* wa = wt + (size_t)ka * YL;
+      const float* wb = wt + (size_t)kb * YL;
+#pragma unroll
+      for (int m = 0; m < 32; ++m) {
+        const int n = j + 64 * m;
+        float a = 0.0f, b = 0.0f;
+        if (m < MNZ && n < YL) {
+          a = __ldg(pa + n * es) * __ldg(wa + n);
+          if (hasb) b = __ldg(pb + n * es) * __ldg(wb + n);
+        }
+        v[m] = make_float2(a, b);
+      }
+    }
+    // ---- A: 32-point DFT over m, twiddle, row j of the buffer --------------
+    dft32_fwd(v);
+#pragma unroll
+    for (int p = 0; p < 32; ++p) {
+      const int k1 = dft32_freq(p);
+      xb[j * kS2 + k1] = cmulw<false>(v[p], twA[k1 * 64 + j]);
+    }
+    bar_pair(pair);
+    // ---- B: column kc, rows of parity e: DFT over j', exchange + filter, inverse
+#pragma unroll
+    for (int q = 0; q < 32; ++q) v[q] = xb[(2 * q + e) * kS2 + kc];
+    dft32_fwd(v);
+    const float sg = e ? -1.0f : 1.0f;  // lane e = 1 multiplies the other lane's E by W_64^-k
+#pragma unroll
+    for (int p = 0; p < 32; ++p) {
+      const int k = dft32_freq(p);
+      const float2 o = make_float2(__shfl_xor_sync(0xffffffffu, v[p].x, 16), __shfl_xor_sync(0xffffffffu, v[p].y, 16));
+      const float2 g = G[k * 32 + kc];
+      const float2 w = c_w64[k];
+      const float wy = sg * w.y;
+      const float2 ow = make_float2(o.x * w.x - o.y * wy, o.x * wy + o.y * w.x);  // o W_64^(+-k)
+      v[p] = make_float2(g.x * v[p].x + g.y * ow.x, g.x * v[p].y + g.y * ow.y);
+    }
+    dft32_inv(v);
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+      const int jj = 2 * q + e;
+      xb[jj * kS2 + kc] = cmulw<true>(v[q], twB[jj * 32 + kc]);
+    }
+    bar_pair(pair);
+    // ---- A': inverse 32-point DFT over k1 of row j: y[j + 64 m] -------------
+#pragma unroll
+    for (int p = 0; p < 32; ++p) v[p] = xb[j * kS2 + dft32_freq(p)];
+    dft32_inv(v);
+    float* oa = out + (size_t)ra * YL;
+    float* ob = out + (size_t)rb * YL;
+#pragma unroll
+    for (int m = 0; m < MNZ; ++m) {
+      const int n = j + 64 * m;
+      if (n < YL) {
+        oa[n] = v[m].x;
+        if (hasb) ob[n] = v[m].y;
+      }
+    }
+  }
+}
+
+size_t smem_bytes2() { return (2 * 32 * 64 + 32 * 32 + kPairs * 64 * kS2) * sizeof(float2); }
+
+template <int IN_LAYOUT, bool STAGE, int MNZ>
+int launch_k2(const hr_filter_plan* p, float* out, const float* in, int view0, cudaStream_t s) {
+  auto kern = filter2048x2_kernel<IN_LAYOUT, STAGE, MNZ>;
+  const size_t smem = smem_bytes2();
+  HR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long rows = (long long)p->ZL * p->ViewN;
+  const long long tiles = ((rows + 1) / 2 + kPairs - 1) / kPairs;
+  int per_sm = 0;
+  HR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads2, smem));
+  if (per_sm < 1) per_sm = 1;
+  const long long want = (long long)per_sm * hr::sm_count();
+  const int grid = (int)(tiles < want ? tiles : want);
+  kern<<<grid, kThreads2, smem, s>>>(out, in, p->d_tw3, p->d_G, STAGE ? p->d_wt8 : p->d_wt, p->YL, p->ZL, rows,
+                                     view0);
+  HR_CUDA_TRY(cudaGetLastError());
+  return HR_OK;
+}
+
+template <int IN_LAYOUT, bool STAGE>
+int launch_k2m(const hr_filter_plan* p, float* out, const float* in, int view0, cudaStream_t s) {
+  if (p->YL <= 64 * 14) return launch_k2<IN_LAYOUT, STAGE, 14>(p, out, in, view0, s);
+  return launch_k2<IN_LAYOUT, STAGE, 16>(p, out, in, view0, s);
+}
+
+template <int IN_LAYOUT>
+int launch2(const hr_filter_plan* p, float* out, const float* in, int view0, cudaStream_t s) {
+  if constexpr (IN_LAYOUT == HR_LAYOUT_REBIN)
+    if (p->ZL % 8 == 0 && ((uintptr_t)in & 15) == 0) return launch_k2m<IN_LAYOUT, true>(p, out, in, view0, s);
+  return launch_k2m<IN_LAYOUT, false>(p, out, in, view0, s);
+}
+
 }  // namespace fft2k
 
 size_t smem_bytes(int log2N) {
@@ -553,7 +751,8 @@ int launch_layout(const hr_filter_plan* p, float* out, const float* in, int view
     case 8: return launch_t<8, IN_LAYOUT>(p, out, in, view0, s);
     case 9: return launch_t<9, IN_LAYOUT>(p, out, in, view0, s);
     case 10: return launch_t<10, IN_LAYOUT>(p, out, in, view0, s);
-    case 11: return fft2k::launch<IN_LAYOUT>(p, out, in, view0, s);
+    case 11: return p->kernel2048 ? fft2k::launch<IN_LAYOUT>(p, out, in, view0, s)
+                                  : fft2k::launch2<IN_LAYOUT>(p, out, in, view0, s);
     case 12: return launch_t<12, IN_LAYOUT>(p, out, in, view0, s);
     default: return hr::fail(HR_ERR_UNSUPPORTED, "filter: transform length 2^%d unsupported", p->log2N);
   }
@@ -584,17 +783,21 @@ extern "C" int hr_filter_plan_create(hr_filter_plan** plan, int YL, int ZL, int 
   std::vector<double> ct(N);
   for (int t = 0; t < N; ++t) ct[t] = std::cos(2.0 * M_PI * t / N);
   std::vector<float> H(N);
+  std::vector<double> Hd(N);
   for (int k = 0; k < N; ++k) {
     double acc = 0.0;
     for (int n = 0; n < N; ++n)
       if (hs[n] != 0.0) acc += hs[n] * ct[(size_t)k * n % N];
-    H[k] = (float)(acc / N);
+    Hd[k] = acc / N;
+    H[k] = (float)Hd[k];
   }
   std::vector<float2> tw(N);
   for (int t = 0; t < N; ++t)
     tw[t] = make_float2((float)std::cos(2.0 * M_PI * t / N), (float)-std::sin(2.0 * M_PI * t / N));
-  hr_filter_plan* p =
-      new hr_filter_plan{YL, ZL, ViewN, log2N, PLC, ZLC, dYL, dZL, SO, nullptr, nullptr, nullptr, nullptr};
+  hr_filter_plan* p = new hr_filter_plan{};
+  p->YL = YL; p->ZL = ZL; p->ViewN = ViewN; p->log2N = log2N;
+  p->PLC = PLC; p->ZLC = ZLC; p->dYL = dYL; p->dZL = dZL; p->SO = SO;
+  if (const char* ev = std::getenv("HELIXRECON_FILTER2048")) p->kernel2048 = std::atoi(ev) == 1 ? 1 : 0;
   cudaError_t e = cudaMalloc(&p->d_H, sizeof(float) * N);
   if (e == cudaSuccess) e = cudaMalloc(&p->d_tw, sizeof(float2) * N);
   if (e == cudaSuccess) e = cudaMemcpy(p->d_H, H.data(), sizeof(float) * N, cudaMemcpyHostToDevice);
@@ -606,12 +809,27 @@ extern "C" int hr_filter_plan_create(hr_filter_plan** plan, int YL, int ZL, int 
       for (int j = 0; j < 32; ++j) tw2[c * 32 + j] = tw[(size_t)c * j];
     for (int x = 0; x < 64; ++x)
       w64[x] = make_float2((float)std::cos(2.0 * M_PI * x / 64), (float)-std::sin(2.0 * M_PI * x / 64));
-    e = cudaMalloc(&p->d_tw2, sizeof(float2) * tw2.size());
+    // the two-warp kernel's tables: W_2048^(j k1) by [k1][j] (k1 < 32, j < 64); the filter folded with the
+    // radix-2 step, {H[k1 + 32 k] + H[k1 + 32 k + 1024], H[k1 + 32 k] - H[k1 + 32 k + 1024]} by [k][k1]
+    std::vector<float2> tw3(32 * 64), G(32 * 32);
+    for (int k1 = 0; k1 < 32; ++k1)
+      for (int j = 0; j < 64; ++j) tw3[k1 * 64 + j] = tw[(size_t)k1 * j];
+    for (int k = 0; k < 32; ++k)
+      for (int k1 = 0; k1 < 32; ++k1) {
+        const double h0 = Hd[k1 + 32 * k], h1 = Hd[k1 + 32 * k + 1024];
+        G[k * 32 + k1] = make_float2((float)(h0 + h1), (float)(h0 - h1));
+      }
+    e = cudaMalloc(&p->d_tw3, sizeof(float2) * tw3.size());
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_G, sizeof(float2) * G.size());
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_tw3, tw3.data(), sizeof(float2) * tw3.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_G, G.data(), sizeof(float2) * G.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_tw2, sizeof(float2) * tw2.size());
     if (e == cudaSuccess) e = cudaMalloc(&p->d_wt, sizeof(float) * (size_t)YL * ZL);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_tw2, tw2.data(), sizeof(float2) * tw2.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(fft2k::c_w64, w64.data(), sizeof(float2) * 64);
+    if (e == cudaSuccess && ZL % 8 == 0) e = cudaMalloc(&p->d_wt8, sizeof(float) * (size_t)YL * ZL);
     if (e == cudaSuccess) {
-      fft2k::preweight_table_kernel<<<64, 256>>>(p->d_wt, YL, ZL, PLC, ZLC, dYL, dZL, SO);
+      fft2k::preweight_table_kernel<<<64, 256>>>(p->d_wt, p->d_wt8, YL, ZL, PLC, ZLC, dYL, dZL, SO);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -620,7 +838,10 @@ extern "C" int hr_filter_plan_create(hr_filter_plan** plan, int YL, int ZL, int 
     cudaFree(p->d_H);
     cudaFree(p->d_tw);
     cudaFree(p->d_tw2);
+    cudaFree(p->d_tw3);
+    cudaFree(p->d_G);
     cudaFree(p->d_wt);
+    cudaFree(p->d_wt8);
     delete p;
     return hr::fail(e == cudaErrorMemoryAllocation ? HR_ERR_OUT_OF_MEMORY : HR_ERR_CUDA, "filter plan: %s",
                     cudaGetErrorString(e));
@@ -653,6 +874,9 @@ extern "C" void hr_filter_plan_destroy(hr_filter_plan* p) {
   cudaFree(p->d_H);
   cudaFree(p->d_tw);
   cudaFree(p->d_tw2);
+  cudaFree(p->d_tw3);
+  cudaFree(p->d_G);
   cudaFree(p->d_wt);
+  cudaFree(p->d_wt8);
   delete p;
 }

@@ -270,7 +270,7 @@ int execute_host_streamed(hr_recon_plan* p, float* h_vol, const float* h_fan, bo
     if (c == nch - 1) f1 = d.ViewN - 1;
     if (f1 + 1 > copied) {
       HR_CUDA_TRY(cudaMemcpyAsync(p->d_fan + copied * per_view, h_fan + copied * per_view,
-                                  (size_t)(f1 + 1 - copied) * per_view * sizeof(float), cudaMemcpyHostToDevice,
+                                  (size_t)(f1 + 1 - copied) * per_view * sizeof(float), cudaMemcpyDefault,
                                   p->scopy));
       copied = f1 + 1;
     }
@@ -294,14 +294,15 @@ int execute_host_streamed(hr_recon_plan* p, float* h_vol, const float* h_fan, bo
       HR_CUDA_TRY(cudaEventRecord(p->ev_bp[r], p->sbp));
     }
   }
-  // volume out, range by range (enqueued last: a copy to pageable memory returns only when it is done)
+  // volume out, range by range (enqueued last: a copy to pageable memory returns only when it is done); the
+  // copies take their direction from the addresses, so h_vol (and h_fan) may also be device memory
   const size_t ld = (size_t)d.bp.ZN * sizeof(float);
   for (size_t j = 0; j < ranges.size(); ++j) {
     const int z0 = ranges[j].b0 * t.nz, z1 = std::min(d.bp.ZN, ranges[j].b1 * t.nz);
     if (z1 <= z0) continue;
     HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->ev_bp[j], 0));
     HR_CUDA_TRY(cudaMemcpy2DAsync(h_vol + z0, ld, p->d_vol + z0, ld, (size_t)(z1 - z0) * sizeof(float),
-                                  (size_t)d.bp.XN * d.bp.YN, cudaMemcpyDeviceToHost, p->sout));
+                                  (size_t)d.bp.XN * d.bp.YN, cudaMemcpyDefault, p->sout));
   }
   for (cudaStream_t st : {p->scopy, p->sf, p->sbp, p->sout}) HR_CUDA_TRY(cudaStreamSynchronize(st));
   *done = true;
@@ -314,7 +315,7 @@ int execute_host_streamed(hr_recon_plan* p, float* h_vol, const float* h_fan, bo
     hr::log("recon: streamed texture scale exceeded, refilling the whole copy");
     HR_TRY(hr::bp_fast_execute(*f, *g, p->d_vol, p->d_pairs, p->stream));
     const size_t nvol = (size_t)d.bp.XN * d.bp.YN * d.bp.ZN;
-    HR_CUDA_TRY(cudaMemcpyAsync(h_vol, p->d_vol, nvol * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
+    HR_CUDA_TRY(cudaMemcpyAsync(h_vol, p->d_vol, nvol * sizeof(float), cudaMemcpyDefault, p->stream));
     HR_CUDA_TRY(cudaStreamSynchronize(p->stream));
   }
   return HR_OK;
@@ -332,9 +333,9 @@ extern "C" int hr_recon_execute_host(hr_recon_plan* p, float* h_vol, const float
   }
   const size_t nfan = (size_t)p->d.YL * p->d.ZL * p->d.ViewN;
   const size_t nvol = (size_t)p->d.bp.XN * p->d.bp.YN * p->d.bp.ZN;
-  HR_CUDA_TRY(cudaMemcpyAsync(p->d_fan, h_fan, nfan * sizeof(float), cudaMemcpyHostToDevice, p->stream));
+  HR_CUDA_TRY(cudaMemcpyAsync(p->d_fan, h_fan, nfan * sizeof(float), cudaMemcpyDefault, p->stream));
   HR_TRY(hr_recon_execute(p, p->d_vol, p->d_fan, p->stream));
-  HR_CUDA_TRY(cudaMemcpyAsync(h_vol, p->d_vol, nvol * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
+  HR_CUDA_TRY(cudaMemcpyAsync(h_vol, p->d_vol, nvol * sizeof(float), cudaMemcpyDefault, p->stream));
   HR_CUDA_TRY(cudaStreamSynchronize(p->stream));
   return HR_OK;
 }

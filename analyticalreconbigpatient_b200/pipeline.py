@@ -83,7 +83,8 @@ class HelicalRecon:
         return vol
 
     def run_host(self, fan, volume=None):
-        """Host arrays (numpy or CPU tensors; pinned for full copy speed). Synchronous."""
+        """Host arrays (numpy or CPU tensors; pinned for full copy speed); either may also be a CUDA
+        tensor (a host fan into a device volume, for instance). Synchronous."""
         s = self.scan
         if volume is None:
             volume = np.empty((s.YN, s.XN, s.ZN), dtype=np.float32)

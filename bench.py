@@ -750,15 +750,15 @@ def run_learned(args, dev, world, rank, barrier, emit=True):
     # the half view is reconstructed with the chosen (fast) form; the plain form beside it
     rh = {"fast": HelicalRecon(half, form=_lib.HR_FORM_FAST, device=dev),
           "plain": HelicalRecon(half, form=_lib.HR_FORM_PLAIN, device=dev)}
-    d_half = torch.empty(h_half.shape, dtype=torch.float32, device=dev)
     v_half = {k: torch.empty((half.YN, half.XN, half.ZN), dtype=torch.float32, device=dev) for k in rh}
     v_out = {k: torch.empty_like(v_half[k]) for k in rh}
     h_out = torch.empty((half.YN, half.XN, half.ZN), dtype=torch.float32, pin_memory=True)
     h_ref = torch.empty_like(h_out, pin_memory=True)
 
     def learned_step(kind):
-        d_half.copy_(h_half, non_blocking=True)
-        rh[kind].run(d_half, v_half[kind])
+        # the C ABI host entry from pinned memory into the device volume the network reads (the fast form
+        # streams the fan in under its rebinning, filtering and backprojection)
+        rh[kind].run_host(h_half, v_half[kind])
         net.apply_volume(v_half[kind], v_out[kind])
         h_out.copy_(v_out[kind], non_blocking=True)
         torch.cuda.synchronize()
@@ -833,7 +833,8 @@ def run_learned(args, dev, world, rank, barrier, emit=True):
                                  "bound by activation traffic (32 channels: 144 FLOP per byte)"},
             "e2e": {"value": upd_half * world / s_learned / 1e9, "unit": "GUPS", "s_per_volume": s_learned,
                     "h2d_bytes_per_step": half.projection_bytes(), "d2h_bytes_per_step": half.volume_bytes(),
-                    "entry": "HelicalRecon.run (fast form) + Corrector.apply_volume, pinned host fan in, volume out"},
+                    "entry": "HelicalRecon.run_host (hr_recon_execute_host, fast form: pinned half-view fan streamed in, "
+                             "volume into device memory) + Corrector.apply_volume, volume out to pinned memory"},
             # per learned step: rebin, split, Toeplitz GEMM, the backprojection's kernels; then per 32-slice
             # chunk the input packing and 8 conv layers
             "gpu_launches": (3 + fast_launches_per_bp(half_desc) + 9 * ((half.ZN + 31) // 32)) * args.steps,

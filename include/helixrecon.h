@@ -260,7 +260,9 @@ int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* desc);
 /* Device pointers: d_fan [ViewN][YL][ZL] float, d_vol [YN][XN][ZN] float. */
 int hr_recon_execute(const hr_recon_plan* plan, float* d_vol, const float* d_fan, void* stream);
 /* Host pointers (pinned for full copy speed): copies the fan data in, runs the
- * chain, copies the volume out; returns when h_vol is written. The fast form
+ * chain, copies the volume out; returns when h_vol is written. Either pointer
+ * may also be device memory (the copies take their direction from the
+ * addresses: a host fan into a device volume, for instance). The fast form
  * streams: the fan crosses the host link in chunks of 1024 views
  * (HELIXRECON_STREAM_CHUNK at plan creation; 0: no streaming) while the chunks
  * that have arrived are rebinned and filtered, z-block ranges are

@@ -171,14 +171,18 @@ def test_filter_refuses_overlapping_buffers(cuda):
     lib.hr_filter_plan_destroy(plan)
 
 
-@pytest.mark.parametrize("ZL", [16, 7])
-def test_filter_2048_both_layouts_vs_fp64_oracle(cuda, ZL):
-    """888 channels transform with 2048 points (the register-resident kernel):
-    both input layouts against the FP64 oracle, every row within 1e-5 (odd ZL:
-    row pairs that straddle two views), and the two layouts give the same bits."""
+@pytest.mark.parametrize("kernel", ["0", "1"])
+@pytest.mark.parametrize("ZL,YL", [(16, 888), (7, 888), (8, 1000)])
+def test_filter_2048_both_layouts_vs_fp64_oracle(cuda, ZL, YL, kernel, monkeypatch):
+    """888 channels transform with 2048 points (the register-resident kernels:
+    two warps per row pair, or one with HELIXRECON_FILTER2048=1): both input
+    layouts against the FP64 oracle, every row within 1e-5 (odd ZL: row pairs
+    that straddle two views; 1000 channels: no samples pruned), and the two
+    layouts give the same bits."""
     import torch
 
-    sc = G.Scan(ZL=ZL, pitch=0.9375)
+    monkeypatch.setenv("HELIXRECON_FILTER2048", kernel)
+    sc = G.Scan(ZL=ZL, YL=YL, pitch=0.9375)
     fa = sc.filter_args()
     nv = 37
     rng = np.random.default_rng(7)
@@ -202,3 +206,4 @@ def test_filter_2048_both_layouts_vs_fp64_oracle(cuda, ZL):
                             fa["SO"])
     err = np.linalg.norm(got_r - ref, axis=-1) / np.maximum(np.linalg.norm(ref, axis=-1), 1e-30)
     assert err.max() < 1e-5, err.max()
+

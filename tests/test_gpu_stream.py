@@ -90,6 +90,10 @@ def test_streamed_host_entry_matches_the_device_entry(cuda, chunk):
         else:
             assert rel_l2(got, ref) < 1e-6, (chunk, pinned, desc)
             assert np.abs(got - ref).max() < 1e-6 * scale, (chunk, pinned, desc)
+    # a host fan into a device volume (the copies take their direction from the addresses)
+    vol_d = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
+    rec.run_host(fan.cpu().pin_memory(), vol_d)
+    assert np.array_equal(vol_d.cpu().numpy(), got), (chunk, desc)
     rec.close()
 
 
