@@ -239,13 +239,36 @@ __device__ __forceinline__ float2 w8(float2 a) {
   return INV ? make_float2((a.x - a.y) * r, (a.x + a.y) * r) : make_float2((a.x + a.y) * r, (a.y - a.x) * r);
 }
 
+// Complex add / subtract as one packed FP32x2 instruction (sm_100): each lane
+// is an IEEE round-to-nearest add, the same bits as two scalar adds.
+__device__ __forceinline__ unsigned long long f2u(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 u2f(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2u(a)), "l"(f2u(b)));
+  return u2f(d);
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2u(a)), "l"(f2u(b)));
+  return u2f(d);
+}
+
 // 4-point DFT of v[O], v[O+S], v[O+2S], v[O+3S], in place, natural order.
 template <bool INV, int O, int S, int L>
 __device__ __forceinline__ void dft4(float2 (&v)[L]) {
-  const float2 t0 = cadd(v[O], v[O + 2 * S]), t1 = csub(v[O], v[O + 2 * S]);
-  const float2 t2 = cadd(v[O + S], v[O + 3 * S]), t3 = rot<INV>(csub(v[O + S], v[O + 3 * S]));
-  v[O] = cadd(t0, t2);
-  v[O + 2 * S] = csub(t0, t2);
+  const float2 t0 = padd(v[O], v[O + 2 * S]), t1 = psub(v[O], v[O + 2 * S]);
+  const float2 t2 = padd(v[O + S], v[O + 3 * S]), t3 = rot<INV>(psub(v[O + S], v[O + 3 * S]));
+  v[O] = padd(t0, t2);
+  v[O + 2 * S] = psub(t0, t2);
   v[O + S] = cadd(t1, t3);
   v[O + 3 * S] = csub(t1, t3);
 }
@@ -258,14 +281,14 @@ __device__ __forceinline__ void dft8(float2 (&v)[L]) {
   const float2 e0 = v[O], e1 = v[O + 2 * S], e2 = v[O + 4 * S], e3 = v[O + 6 * S];
   const float2 o0 = v[O + S], o1 = w8<INV>(v[O + 3 * S]), o2 = rot<INV>(v[O + 5 * S]);
   const float2 o3 = rot<INV>(w8<INV>(v[O + 7 * S]));
-  v[O] = cadd(e0, o0);
-  v[O + 4 * S] = csub(e0, o0);
-  v[O + S] = cadd(e1, o1);
-  v[O + 5 * S] = csub(e1, o1);
+  v[O] = padd(e0, o0);
+  v[O + 4 * S] = psub(e0, o0);
+  v[O + S] = padd(e1, o1);
+  v[O + 5 * S] = psub(e1, o1);
   v[O + 2 * S] = cadd(e2, o2);
   v[O + 6 * S] = csub(e2, o2);
-  v[O + 3 * S] = cadd(e3, o3);
-  v[O + 7 * S] = csub(e3, o3);
+  v[O + 3 * S] = padd(e3, o3);
+  v[O + 7 * S] = psub(e3, o3);
 }
 
 template <bool INV, int M2>
