@@ -289,13 +289,12 @@ template <int IN_LAYOUT>
 __global__ void __launch_bounds__(256) prep_split_kernel(__nv_bfloat162* __restrict__ a0,
                                                          __nv_bfloat162* __restrict__ a1,
                                                          __nv_bfloat162* __restrict__ a2,
-                                                         const float* __restrict__ in, int YL, int ZL, int KP,
-                                                         int nviews, int view0, float PLC, float ZLC, float dYL,
-                                                         float dZL, float SO) {
+                                                         const float* __restrict__ in,
+                                                         const float2* __restrict__ wt, int YL, int ZL, int KP,
+                                                         int nviews, int view0) {
   __shared__ float tile[64][33];  // [j][k]
   const int j0 = blockIdx.x * 64, k0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  const float SO2 = SO * SO;
   for (long long v = blockIdx.z; v < nviews; v += gridDim.z) {  // uniform over the CTA
     if (v != blockIdx.z) __syncthreads();                        // the previous view's tile has been read
     if (IN_LAYOUT == HR_LAYOUT_REBIN) {
@@ -317,17 +316,8 @@ __global__ void __launch_bounds__(256) prep_split_kernel(__nv_bfloat162* __restr
     for (int yy = ty; yy < 32; yy += 8) {
       const int k = k0 + yy, j = j0 + 2 * tx;
       if (k >= ZL || j >= KP) continue;  // KP is a multiple of 64: j + 1 < KP too
-      const float b = ((float)k - ZLC) * dZL;
-      float x[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        x[h] = 0.0f;
-        if (j + h < YL) {
-          const float t = ((float)(j + h) - PLC) * dYL;
-          const float wei = SO2 / sqrtf(SO2 * (SO2 + b * b) - b * t * b * t);
-          x[h] = tile[2 * tx + h][yy] * wei;
-        }
-      }
+      const float2 w = __ldg(wt + (((size_t)k * KP + j) >> 1));  // the preweights of channels j, j+1 (0 beyond YL)
+      float x[2] = {tile[2 * tx][yy] * w.x, tile[2 * tx + 1][yy] * w.y};
       __nv_bfloat16 p0[2], p1[2], p2[2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
@@ -399,6 +389,7 @@ struct hr_filter_tc_plan {
   long long rows;
   __nv_bfloat16* d_a[kParts];
   __nv_bfloat16* d_t[kParts];
+  float* d_wt;  // cosine preweights [ZL][KP] (0 for channels >= YL), the reference's float expression
   int* d_err;
   CUtensorMap m_a[kParts], m_t[kParts];
   size_t bytes;
@@ -413,6 +404,7 @@ static void tc_destroy(hr_filter_tc_plan* p) {
     if (p->owns_a) cudaFree(p->d_a[i]);
     cudaFree(p->d_t[i]);
   }
+  cudaFree(p->d_wt);
   cudaFree(p->d_err);
   delete p;
 }
@@ -460,8 +452,20 @@ static int tc_create(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float 
       }
     }
   const size_t abytes = (size_t)rows * p->KP * 2, tbytes = (size_t)p->TR * p->KP * 2;
+  // preweights (src/filtering.cu:187-207, in float as there)
+  std::vector<float> wt((size_t)ZL * p->KP, 0.0f);
+  const float SO2 = SO * SO;
+  for (int k = 0; k < ZL; ++k) {
+    const float b = ((float)k - ZLC) * dZL;
+    for (int j = 0; j < YL; ++j) {
+      const float t = ((float)j - PLC) * dYL;
+      wt[(size_t)k * p->KP + j] = SO2 / std::sqrt(SO2 * (SO2 + b * b) - b * t * b * t);
+    }
+  }
   int st = HR_OK;
   cudaError_t e = cudaMalloc(&p->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&p->d_wt, sizeof(float) * wt.size());
+  if (e == cudaSuccess) e = cudaMemcpy(p->d_wt, wt.data(), sizeof(float) * wt.size(), cudaMemcpyHostToDevice);
   for (int i = 0; i < kParts && e == cudaSuccess; ++i) {
     if (ext)
       p->d_a[i] = static_cast<__nv_bfloat16*>(ext[i]);
@@ -482,7 +486,7 @@ static int tc_create(hr_filter_tc_plan** plan, int YL, int ZL, int ViewN, float 
     tc_destroy(p);
     return st;
   }
-  p->bytes = kParts * ((ext ? 0 : abytes) + tbytes) + sizeof(int);
+  p->bytes = kParts * ((ext ? 0 : abytes) + tbytes) + sizeof(int) + sizeof(float) * wt.size();
   *plan = p;
   return HR_OK;
 }
@@ -523,11 +527,11 @@ int hr::filter_tc_execute_limited(const hr_filter_tc_plan* p, uint32_t* d_pairs,
   auto* a1 = reinterpret_cast<__nv_bfloat162*>(p->d_a[1]);
   auto* a2 = reinterpret_cast<__nv_bfloat162*>(p->d_a[2]);
   if (in_layout == HR_LAYOUT_REBIN)
-    prep_split_kernel<HR_LAYOUT_REBIN><<<pgrid, 256, 0, s>>>(a0, a1, a2, d_in, p->YL, p->ZL, p->KP, p->ViewN, view0,
-                                                             p->PLC, p->ZLC, p->dYL, p->dZL, p->SO);
+    prep_split_kernel<HR_LAYOUT_REBIN><<<pgrid, 256, 0, s>>>(a0, a1, a2, d_in, reinterpret_cast<const float2*>(p->d_wt),
+                                                             p->YL, p->ZL, p->KP, p->ViewN, view0);
   else
-    prep_split_kernel<HR_LAYOUT_ROWS><<<pgrid, 256, 0, s>>>(a0, a1, a2, d_in, p->YL, p->ZL, p->KP, p->ViewN, view0,
-                                                            p->PLC, p->ZLC, p->dYL, p->dZL, p->SO);
+    prep_split_kernel<HR_LAYOUT_ROWS><<<pgrid, 256, 0, s>>>(a0, a1, a2, d_in, reinterpret_cast<const float2*>(p->d_wt),
+                                                            p->YL, p->ZL, p->KP, p->ViewN, view0);
   HR_CUDA_TRY(cudaGetLastError());
   const size_t smem = (size_t)kStages * kStageBytes + 1024 + 128;
   HR_CUDA_TRY(cudaFuncSetAttribute(toeplitz_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
