@@ -730,6 +730,18 @@ __global__ void __launch_bounds__(kBx* kBy) bp_tex_seg_kernel(float* __restrict_
   tex_seg_column<NZ, V>(vol, X, T, P, xi, yi, b_first + blockIdx.z);
 }
 
+// The same column code with registers bounded for 6 CTAs of 256 threads per
+// SM (40 registers instead of 48: one CTA more per SM to hide the texture
+// latency).
+template <int NZ, int V>
+__global__ void __launch_bounds__(kBx* kBy, 6) bp_tex_seg6_kernel(float* __restrict__ vol, const TexRef X,
+                                                                 const ZTabs T, const FastParams P, int b_first) {
+  const int xi = blockIdx.x * kBx + threadIdx.x;
+  const int yi = blockIdx.y * kBy + threadIdx.y;
+  if (xi >= P.XN || yi >= P.YN) return;
+  tex_seg_column<NZ, V>(vol, X, T, P, xi, yi, b_first + blockIdx.z);
+}
+
 // The persistent multi-scan launch with texture taps: the work items and
 // their claiming as in bp_fast_batch_kernel; each scan samples its own arrays
 // with 8 or 4 slices per thread (NZF = 0: the scan's own choice) or 4 for all
@@ -1186,9 +1198,12 @@ static void launch_tex(const BpFastTables& t, const BpFast& f, const FastParams&
 
 template <int NZ, int V>
 static void launch_tex_seg(const BpFastTables& t, const BpFast& f, const FastParams& P, float* vol, int b_first,
-                           int b_count, cudaStream_t s) {
+                           int b_count, bool occ6, cudaStream_t s) {
   dim3 grid((P.XN + kBx - 1) / kBx, (P.YN + kBy - 1) / kBy, b_count);
-  bp_tex_seg_kernel<NZ, V><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), P, b_first);
+  if (occ6)
+    bp_tex_seg6_kernel<NZ, V><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), P, b_first);
+  else
+    bp_tex_seg_kernel<NZ, V><<<grid, dim3(kBx, kBy), 0, s>>>(vol, texref(f), ztabs(t, f), P, b_first);
 }
 
 // Launches variant v over z blocks [b_first, b_first + b_count) (count < 0: all).
@@ -1204,13 +1219,13 @@ static int run_variant(const BpFast& f, const BpFastGeom& g, int v, float* vol, 
     HR_REQUIRE(f.tex.kind == fv.tex && f.tex.views >= g.PN, "fast backprojection: the textures of variant %d are "
                "not prepared", v);
     if (fv.seg) {
-      const bool two = fv.seg == 2;
+      const bool two = fv.seg == 2, occ6 = fv.occ == 6;
       if (kFastNz[fv.table] == 8)
-        two ? launch_tex_seg<8, 2>(t, f, P, vol, b_first, b_count, s)
-            : launch_tex_seg<8, 1>(t, f, P, vol, b_first, b_count, s);
+        two ? launch_tex_seg<8, 2>(t, f, P, vol, b_first, b_count, occ6, s)
+            : launch_tex_seg<8, 1>(t, f, P, vol, b_first, b_count, occ6, s);
       else
-        two ? launch_tex_seg<4, 2>(t, f, P, vol, b_first, b_count, s)
-            : launch_tex_seg<4, 1>(t, f, P, vol, b_first, b_count, s);
+        two ? launch_tex_seg<4, 2>(t, f, P, vol, b_first, b_count, occ6, s)
+            : launch_tex_seg<4, 1>(t, f, P, vol, b_first, b_count, occ6, s);
     } else {
       switch (kFastNz[fv.table]) {
         case 16: launch_tex<16>(t, f, P, vol, b_first, b_count, s); break;
@@ -1495,8 +1510,10 @@ int bp_fast_describe(const BpFast& f, char* buf, int len) {
   if (!buf || len <= 0) return HR_OK;
   const FastVariant& fv = kFastVariants[f.variant];
   int n = snprintf(buf, (size_t)len, "slices_per_thread=%d gathers=%s tile=%dx%d %s", kFastNz[fv.table],
-                   fv.tex == kTexHalf ? (fv.seg == 2 ? "texture-fp16-segmented-two-views"
-                                        : fv.seg ? "texture-fp16-segmented" : "texture-fp16")
+                   fv.tex == kTexHalf ? (fv.seg == 2 ? (fv.occ ? "texture-fp16-segmented-two-views-6ctas"
+                                                               : "texture-fp16-segmented-two-views")
+                                        : fv.seg ? (fv.occ ? "texture-fp16-segmented-6ctas" : "texture-fp16-segmented")
+                                        : "texture-fp16")
                    : fv.tex == kTexFloat ? "texture-fp32"
                    : fv.chunk < 0 ? "paired-f32x2" : fv.chunk == 0 ? "per-slice" : fv.chunk == 4 ? "chunk4" : "chunk8",
                    kBx, kBy, f.tuned == 2 ? "(pinned by HELIXRECON_BP_VARIANT)"

@@ -35,16 +35,18 @@ constexpr int kTexHalf = 1, kTexFloat = 2;
 // slices without the view cost nothing (thick slices: a block's union window
 // is much longer than one slice's); seg = 2: segments whose range holds at
 // most 4 slices run two views per iteration, both views' taps in flight
-// together (thick slices: few taps per view).
+// together (thick slices: few taps per view). occ = 6: the segmented code with
+// registers bounded for 6 CTAs per SM.
 struct FastVariant {
-  int table, chunk, tex, seg;
+  int table, chunk, tex, seg, occ;
 };
 constexpr FastVariant kFastVariants[] = {{0, 0}, {0, 4}, {0, 8}, {1, 0}, {1, 4}, {1, 8},
                                          {0, -1}, {1, -1}, {2, 0}, {2, -1}, {2, 4},
                                          {1, 0, kTexHalf}, {0, 0, kTexHalf}, {2, 0, kTexHalf},
                                          {1, 0, kTexFloat}, {0, 0, kTexFloat},
                                          {1, 0, kTexHalf, 1}, {2, 0, kTexHalf, 1},
-                                         {1, 0, kTexHalf, 2}, {2, 0, kTexHalf, 2}};
+                                         {1, 0, kTexHalf, 2}, {2, 0, kTexHalf, 2},
+                                         {1, 0, kTexHalf, 1, 6}, {2, 0, kTexHalf, 2, 6}};
 constexpr int kFastVariants_n = sizeof(kFastVariants) / sizeof(kFastVariants[0]);
 constexpr int kFastDefaultVariant = 0;
 

@@ -210,7 +210,7 @@ extern "C" int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* d
     return st;
   }
   if (hr::log_enabled()) {
-    char desc[512];
+    char desc[1024];
     if (hr_recon_describe(p, desc, sizeof(desc)) == HR_OK)
       hr::log("recon plan: %d views -> %dx%dx%d, %.2f GB on the device; %s", d->ViewN, d->bp.XN, d->bp.YN, d->bp.ZN,
               hr_recon_device_bytes(p) / 1e9, desc);
@@ -221,7 +221,7 @@ extern "C" int hr_recon_plan_create(hr_recon_plan** plan, const hr_recon_desc* d
 
 extern "C" int hr_recon_describe(const hr_recon_plan* p, char* buf, int len) {
   HR_REQUIRE(p != nullptr, "hr_recon_describe: NULL plan");
-  char bp[400];
+  char bp[640];
   HR_TRY(hr_bp_describe(p->bp, bp, sizeof(bp)));
   if (buf && len > 0)
     snprintf(buf, (size_t)len, "filter=%s; backprojection: %s",

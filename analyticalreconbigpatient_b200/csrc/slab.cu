@@ -377,7 +377,7 @@ static int prepare(hr_slab_plan* p, const float* fan, int fan_view0, bool fan_on
     HR_TRY(capture(p, bb, p->sc, slab_bp, &p->gbp[bb]));
   }
   if (hr::log_enabled()) {
-    char desc[768];
+    char desc[1024];
     if (hr_slab_describe(p, desc, sizeof(desc)) == HR_OK) hr::log("slab plan prepared: %s", desc);
   }
   return HR_OK;
@@ -441,7 +441,7 @@ extern "C" int hr_slab_fan_range(const hr_slab_plan* p, int* first_view, int* nv
 
 extern "C" int hr_slab_describe(const hr_slab_plan* p, char* buf, int len) {
   HR_REQUIRE(p != nullptr, "hr_slab_describe: NULL plan");
-  char bp[384];
+  char bp[640];
   HR_TRY(hr::bp_fast_describe(p->fast[0], bp, sizeof(bp)));
   if (buf && len > 0) {
     char part[96] = "";

@@ -69,8 +69,8 @@ class HelicalRecon:
         _lib.check(_lib.load().hr_recon_check(self._plan))
 
     def describe(self) -> str:
-        buf = ctypes.create_string_buffer(512)
-        _lib.check(_lib.load().hr_recon_describe(self._plan, buf, 512))
+        buf = ctypes.create_string_buffer(1024)
+        _lib.check(_lib.load().hr_recon_describe(self._plan, buf, 1024))
         return buf.value.decode()
 
     def run(self, fan: torch.Tensor, volume: torch.Tensor | None = None, stream=None) -> torch.Tensor:
@@ -196,8 +196,8 @@ class SlabRecon:
             _lib.check(_lib.load().hr_slab_execute_range(self._plan, vp, fp, fan_view0, vh, fh))
 
     def describe(self) -> str:
-        buf = ctypes.create_string_buffer(768)
-        _lib.check(_lib.load().hr_slab_describe(self._plan, buf, 768))
+        buf = ctypes.create_string_buffer(1024)
+        _lib.check(_lib.load().hr_slab_describe(self._plan, buf, 1024))
         return buf.value.decode()
 
     @property
@@ -279,8 +279,8 @@ class BatchRecon:
         _lib.check(_lib.load().hr_batch_check(self._plan))
 
     def describe(self) -> str:
-        buf = ctypes.create_string_buffer(768)
-        _lib.check(_lib.load().hr_batch_describe(self._plan, buf, 768))
+        buf = ctypes.create_string_buffer(1024)
+        _lib.check(_lib.load().hr_batch_describe(self._plan, buf, 1024))
         return buf.value.decode()
 
     @property
@@ -342,8 +342,8 @@ class StagePlans:
     def autotune(self, vol: torch.Tensor, fp: torch.Tensor, stream: int = 0) -> str:
         lib = _lib.load()
         _lib.check(lib.hr_bp_autotune(self._bp, vol.data_ptr(), fp.data_ptr(), stream))
-        buf = ctypes.create_string_buffer(512)
-        _lib.check(lib.hr_bp_describe(self._bp, buf, 512))
+        buf = ctypes.create_string_buffer(1024)
+        _lib.check(lib.hr_bp_describe(self._bp, buf, 1024))
         return buf.value.decode()
 
     def pack(self, out: torch.Tensor, filtered: torch.Tensor, stream: int = 0) -> None:

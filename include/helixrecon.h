@@ -210,7 +210,8 @@ int hr_bp_describe(const hr_bp_plan* plan, char* buf, int len);
  * from the FP16 copy with the view loop cut into segments of a fixed set of
  * slices holding the view (thick slices), 18-19 eight / four slices per
  * thread as 16-17 with two views per iteration in segments of at most four
- * slices (thick slices: more taps in flight); the texture variants allocate the
+ * slices (thick slices: more taps in flight), 20 as 16 and 21 as 19 with
+ * registers bounded for 6 CTAs per SM; the texture variants allocate the
  * copy, 2 or 4 bytes per sample, and fill it on every execution).
  * For tests and manual tuning. */
 int hr_bp_select(hr_bp_plan* plan, int variant);

@@ -127,7 +127,7 @@ def test_every_fast_variant_gives_the_same_volume(cuda, pixel):
     fast.pack(pairs, filt)
     lib = _lib.load()
     vols = []
-    nvar = 20
+    nvar = 22
     for v in range(nvar):
         _lib.check(lib.hr_bp_select(fast._bp, v))
         vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
@@ -152,6 +152,8 @@ def test_every_fast_variant_gives_the_same_volume(cuda, pixel):
     # segments): same operations per slice and view, in the same order
     assert np.array_equal(vols[16], vols[11]) and np.array_equal(vols[17], vols[13])
     assert np.array_equal(vols[18], vols[11]) and np.array_equal(vols[19], vols[13])
+    # 20, 21: the code of 16 and 19 with registers bounded for 6 CTAs per SM
+    assert np.array_equal(vols[20], vols[16]) and np.array_equal(vols[21], vols[19])
     assert np.isfinite(vols[0]).all()
 
 
@@ -172,7 +174,7 @@ def test_two_view_segments_equal_one_view_at_thick_slices(cuda):
     fast.pack(pairs, filt)
     lib = _lib.load()
     vols = {}
-    for v in (11, 13, 16, 17, 18, 19):
+    for v in (11, 13, 16, 17, 18, 19, 20, 21):
         _lib.check(lib.hr_bp_select(fast._bp, v))
         vol = torch.full((sc.YN, sc.XN, sc.ZN), float("nan"), device=cuda)
         fast.backproject(vol, pairs)
@@ -180,7 +182,7 @@ def test_two_view_segments_equal_one_view_at_thick_slices(cuda):
         vols[v] = vol.cpu().numpy()
     fast.close()
     assert np.isfinite(vols[11]).all() and np.count_nonzero(vols[11]) > vols[11].size // 2
-    for a, b in ((18, 11), (16, 11), (19, 13), (17, 13)):
+    for a, b in ((18, 11), (16, 11), (19, 13), (17, 13), (20, 11), (21, 13)):
         assert np.array_equal(vols[a], vols[b]), (a, b)
 
 
