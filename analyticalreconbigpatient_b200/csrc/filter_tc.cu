@@ -19,14 +19,17 @@
 // Stages:
 //   1. prep kernel: rebinned (or row-layout) FP32 -> preweighted, split,
 //      K-major BF16 rows A0/A1/A2 [rows][KP] (KP = YL rounded up to 64).
-//   2. GEMM kernel, one CTA per (128-row, 112-column) output tile, 4 warps:
-//      warp 0 lane 0 issues TMA loads of A0..A2 (128 x 64) and T0..T2
-//      (128 x 64; 16 extra columns give every pair its right neighbour) into
-//      a 2-stage ring of 128B-swizzled shared-memory tiles; warp 1 lane 0
-//      issues 24 tcgen05.mma (M=128, N=128, K=16) per 64-wide K block into a
-//      TMEM accumulator of 128 FP32 columns and commits each stage back to the
-//      producer; after the last block all 4 warps read their 32 TMEM lanes
-//      (tcgen05.ld 32x32b) and store BF16 pairs.
+//   2. GEMM kernel, persistent (one CTA of 6 warps per SM walking the
+//      (128-row, 112-column) output tiles): warp 0 lane 0 issues TMA loads of
+//      A0..A2 (128 x 64) and T0..T2 (128 x 64; 16 extra columns give every
+//      pair its right neighbour) into a 2-stage ring of 128B-swizzled
+//      shared-memory tiles, across tile boundaries; warp 1 lane 0 issues 24
+//      tcgen05.mma (M=128, N=128, K=16) per 64-wide K block into one of two
+//      TMEM accumulators of 128 FP32 columns (alternating by tile) and
+//      commits each stage back to the producer and each finished tile to the
+//      epilogue; warps 2-5 read their 32 TMEM lanes each (tcgen05.ld 32x32b),
+//      store BF16 pairs and release the accumulator, so that a tile's
+//      epilogue runs under the next tile's MMAs.
 // Every mbarrier wait is bounded: on timeout the kernel records an error in a
 // device flag, stops issuing, lets committed work drain, frees its TMEM and
 // returns; hr_filter_tc_check reports the flag.
@@ -51,8 +54,9 @@ constexpr int kTileA = kBM * kBK * 2;          // 16 KiB
 constexpr int kTileB = kBN * kBK * 2;          // 16 KiB
 constexpr int kParts = 3;                      // BF16 parts per operand
 constexpr int kStageBytes = kParts * kTileA + kParts * kTileB;
-constexpr int kTmemCols = 128;
-constexpr int kThreads = 128;
+constexpr int kEpiWarps = 4;                   // epilogue warps (one per TMEM lane quarter)
+constexpr int kTmemCols = 2 * kBN;             // two accumulators
+constexpr int kThreads = 32 * (2 + kEpiWarps); // producer warp, MMA warp, epilogue warps
 constexpr uint32_t kWaitLimit = 1u << 20;      // try_wait rounds before a wait is declared hung
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -159,30 +163,45 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
   return a | (b << 16);
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Persistent: one CTA per SM walks the output tiles blockIdx.x, + gridDim.x, ...
+// (column tiles of a row tile consecutive). Warp 0 streams the tiles' K blocks
+// through the shared-memory ring; warp 1 accumulates each tile into one of two
+// TMEM accumulators, alternately, and commits it to tfull; warps 2-5 (each
+// reading its own quarter of the TMEM lanes) store a finished accumulator as
+// BF16 channel pairs and hand it back through tempty, so a tile's epilogue runs
+// under the next tile's MMAs. Per output element the products are accumulated
+// in the same order as before, so the values are the same.
 __global__ void __launch_bounds__(kThreads, 1)
     toeplitz_tc_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmA1,
                        const __grid_constant__ CUtensorMap tmA2, const __grid_constant__ CUtensorMap tmT0,
                        const __grid_constant__ CUtensorMap tmT1, const __grid_constant__ CUtensorMap tmT2,
                        uint32_t* __restrict__ out, long long rows, int YL, int n_tiles, int k_blocks,
-                       int* __restrict__ err, int stall_kb, uint32_t wait_limit) {
+                       long long n_work, int* __restrict__ err, int stall_kb, uint32_t wait_limit) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accb = empty + kStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
+  uint64_t* tfull = empty + kStages;  // [2] accumulator b holds a finished tile
+  uint64_t* tempty = tfull + 2;       // [2] accumulator b has been read out
+  uint64_t* drained = tempty + 2;     // the MMA issuer's own operations have completed (abort path)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long m0 = (long long)(blockIdx.x / n_tiles) * kBM;
-  const int n0 = (blockIdx.x % n_tiles) * kBNOut;
-
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accb, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], kEpiWarps);
+    }
+    mbar_init(drained, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -196,83 +215,119 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0 && lane == 0) {
-    // ---- producer: TMA loads ----------------------------------------------
-    int last_kb[kStages];
-    for (int s = 0; s < kStages; ++s) last_kb[s] = -1;
-    for (int kb = 0; kb < k_blocks; ++kb) {
-      const int s = kb % kStages;
-      if (kb >= kStages && !mbar_wait(&empty[s], ((kb / kStages) - 1) & 1, err, abort_flag, wait_limit)) break;
-      if (kb == stall_kb) continue;  // test hook: this block's stage is never filled
-      last_kb[s] = kb;
-      uint8_t* st = smem + s * kStageBytes;
-      mbar_expect_tx(&full[s], kStageBytes);
-      tma_load_2d(st, &tmA0, &full[s], kb * kBK, (int)m0);
-      tma_load_2d(st + kTileA, &tmA1, &full[s], kb * kBK, (int)m0);
-      tma_load_2d(st + 2 * kTileA, &tmA2, &full[s], kb * kBK, (int)m0);
-      tma_load_2d(st + 3 * kTileA, &tmT0, &full[s], kb * kBK, n0);
-      tma_load_2d(st + 3 * kTileA + kTileB, &tmT1, &full[s], kb * kBK, n0);
-      tma_load_2d(st + 3 * kTileA + 2 * kTileB, &tmT2, &full[s], kb * kBK, n0);
+    // ---- producer: TMA loads of every K block of every tile -----------------
+    long long last_g[kStages];
+    for (int s = 0; s < kStages; ++s) last_g[s] = -1;
+    long long g = 0;  // K blocks issued over the CTA's tiles
+    bool ok = true;
+    for (long long t = blockIdx.x; t < n_work && ok; t += gridDim.x) {
+      const int m0 = (int)(t / n_tiles) * kBM, n0 = (int)(t % n_tiles) * kBNOut;
+      for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+        const int s = (int)(g % kStages);
+        if (g >= kStages && !mbar_wait(&empty[s], (uint32_t)((g / kStages) - 1) & 1, err, abort_flag, wait_limit)) {
+          ok = false;
+          break;
+        }
+        if (kb == stall_kb) continue;  // test hook: this block's stage is never filled
+        last_g[s] = g;
+        uint8_t* st = smem + s * kStageBytes;
+        mbar_expect_tx(&full[s], kStageBytes);
+        tma_load_2d(st, &tmA0, &full[s], kb * kBK, m0);
+        tma_load_2d(st + kTileA, &tmA1, &full[s], kb * kBK, m0);
+        tma_load_2d(st + 2 * kTileA, &tmA2, &full[s], kb * kBK, m0);
+        tma_load_2d(st + 3 * kTileA, &tmT0, &full[s], kb * kBK, n0);
+        tma_load_2d(st + 3 * kTileA + kTileB, &tmT1, &full[s], kb * kBK, n0);
+        tma_load_2d(st + 3 * kTileA + 2 * kTileB, &tmT2, &full[s], kb * kBK, n0);
+      }
     }
     // every issued copy has landed before the CTA can exit (after an abort nobody consumes them)
     for (int s = 0; s < kStages; ++s)
-      if (last_kb[s] >= 0) mbar_drain(&full[s], (last_kb[s] / kStages) & 1, err, wait_limit);
+      if (last_g[s] >= 0) mbar_drain(&full[s], (uint32_t)(last_g[s] / kStages) & 1, err, wait_limit);
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----------------------------------------------------------
-    for (int kb = 0; kb < k_blocks; ++kb) {
-      const int s = kb % kStages;
-      if (!mbar_wait(&full[s], (kb / kStages) & 1, err, abort_flag, wait_limit)) break;
+    long long g = 0;
+    bool ok = true, issued = false;
+    int i = 0;  // tiles of this CTA
+    for (long long t = blockIdx.x; t < n_work && ok; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      if (i >= 2 && !mbar_wait(&tempty[b], (uint32_t)((i >> 1) - 1) & 1, err, abort_flag, wait_limit)) {
+        ok = false;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint8_t* st = smem + s * kStageBytes;
-      const uint64_t a0 = umma_desc_sw128(st), a1 = umma_desc_sw128(st + kTileA),
-                     a2 = umma_desc_sw128(st + 2 * kTileA);
-      const uint64_t t0 = umma_desc_sw128(st + 3 * kTileA), t1 = umma_desc_sw128(st + 3 * kTileA + kTileB),
-                     t2 = umma_desc_sw128(st + 3 * kTileA + 2 * kTileB);
-#pragma unroll
-      for (int kk = 0; kk < kBK / 16; ++kk) {
-        const uint64_t step = (uint64_t)(kk * 32) >> 4;  // 16 BF16 = 32 bytes along K
-        // smallest terms first, so that they are not absorbed by the large ones
-        umma_bf16(tmem, a2 + step, t0 + step, (kb | kk) ? 1u : 0u);
-        umma_bf16(tmem, a1 + step, t1 + step, 1u);
-        umma_bf16(tmem, a0 + step, t2 + step, 1u);
-        umma_bf16(tmem, a1 + step, t0 + step, 1u);
-        umma_bf16(tmem, a0 + step, t1 + step, 1u);
-        umma_bf16(tmem, a0 + step, t0 + step, 1u);
-      }
-      umma_commit(&empty[s]);
-    }
-    umma_commit(accb);  // arrives when every MMA issued above has completed
-  }
-  __syncwarp();
-
-  // ---- epilogue: TMEM -> BF16 channel pairs --------------------------------
-  const bool waited = mbar_wait(accb, 0, err, abort_flag, wait_limit);
-  // tcgen05.ld is warp-collective: the whole warp reads TMEM or none of it does
-  const bool acc_ok = __all_sync(0xffffffffu, waited && !*abort_flag);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const long long row = m0 + warp * 32 + lane;
-  const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-  if (acc_ok) {
-    float cur[8], nxt[8];
-    tmem_ld8(taddr, cur);
-    uint32_t* orow = out + row * (long long)YL;
-#pragma unroll 1
-    for (int c = 0; c < kBNOut / 8; ++c) {
-      tmem_ld8(taddr + (uint32_t)((c + 1) * 8), nxt);
-      const int j0 = n0 + c * 8;
-      if (row < rows) {
-        uint32_t w[8];
-#pragma unroll
-        for (int i = 0; i < 7; ++i) w[i] = pack_bf16x2(cur[i], cur[i + 1]);
-        w[7] = pack_bf16x2(cur[7], nxt[0]);
-        if (j0 + 8 <= YL && (YL & 3) == 0) {  // row starts are 16-byte aligned only if YL % 4 == 0
-          reinterpret_cast<uint4*>(orow + j0)[0] = make_uint4(w[0], w[1], w[2], w[3]);
-          reinterpret_cast<uint4*>(orow + j0)[1] = make_uint4(w[4], w[5], w[6], w[7]);
-        } else {
-          for (int i = 0; i < 8 && j0 + i < YL; ++i) orow[j0 + i] = w[i];
+      const uint32_t acc = tmem + (uint32_t)(b * kBN);
+      for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+        const int s = (int)(g % kStages);
+        if (!mbar_wait(&full[s], (uint32_t)(g / kStages) & 1, err, abort_flag, wait_limit)) {
+          ok = false;
+          break;
         }
-      }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint8_t* st = smem + s * kStageBytes;
+        const uint64_t a0 = umma_desc_sw128(st), a1 = umma_desc_sw128(st + kTileA),
+                       a2 = umma_desc_sw128(st + 2 * kTileA);
+        const uint64_t t0 = umma_desc_sw128(st + 3 * kTileA), t1 = umma_desc_sw128(st + 3 * kTileA + kTileB),
+                       t2 = umma_desc_sw128(st + 3 * kTileA + 2 * kTileB);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) cur[i] = nxt[i];
+        for (int kk = 0; kk < kBK / 16; ++kk) {
+          const uint64_t step = (uint64_t)(kk * 32) >> 4;  // 16 BF16 = 32 bytes along K
+          // smallest terms first, so that they are not absorbed by the large ones
+          umma_bf16(acc, a2 + step, t0 + step, (kb | kk) ? 1u : 0u);
+          umma_bf16(acc, a1 + step, t1 + step, 1u);
+          umma_bf16(acc, a0 + step, t2 + step, 1u);
+          umma_bf16(acc, a1 + step, t0 + step, 1u);
+          umma_bf16(acc, a0 + step, t1 + step, 1u);
+          umma_bf16(acc, a0 + step, t0 + step, 1u);
+        }
+        umma_commit(&empty[s]);
+        issued = true;
+      }
+      if (ok) umma_commit(&tfull[b]);  // arrives when every MMA of the tile has completed
+    }
+    // after an abort, the tensor core finishes what was issued before the TMEM is freed
+    if (!ok && issued) {
+      umma_commit(drained);
+      mbar_drain(drained, 0, err, wait_limit);
+    }
+  } else if (warp >= 2) {
+    // ---- epilogue: TMEM -> BF16 channel pairs, tile after tile -----------------
+    const int q = warp & 3;  // the TMEM lane quarter this warp may read
+    int i = 0;
+    for (long long t = blockIdx.x; t < n_work; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      const bool waited = mbar_wait(&tfull[b], (uint32_t)(i >> 1) & 1, err, abort_flag, wait_limit);
+      // tcgen05.ld is warp-collective: the whole warp reads TMEM or none of it does
+      if (!__all_sync(0xffffffffu, waited && !*abort_flag)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const long long m0 = (t / n_tiles) * kBM;
+      const int n0 = (int)(t % n_tiles) * kBNOut;
+      const long long row = m0 + q * 32 + lane;
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kBN);
+      float cur[8], nxt[8];
+      tmem_ld8(taddr, cur);
+      uint32_t* orow = out + row * (long long)YL;
+#pragma unroll 1
+      for (int c = 0; c < kBNOut / 8; ++c) {
+        tmem_ld8(taddr + (uint32_t)((c + 1) * 8), nxt);
+        const int j0 = n0 + c * 8;
+        if (row < rows) {
+          uint32_t w[8];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) w[k] = pack_bf16x2(cur[k], cur[k + 1]);
+          w[7] = pack_bf16x2(cur[7], nxt[0]);
+          if (j0 + 8 <= YL && (YL & 3) == 0) {  // row starts are 16-byte aligned only if YL % 4 == 0
+            reinterpret_cast<uint4*>(orow + j0)[0] = make_uint4(w[0], w[1], w[2], w[3]);
+            reinterpret_cast<uint4*>(orow + j0)[1] = make_uint4(w[4], w[5], w[6], w[7]);
+          } else {
+            for (int k = 0; k < 8 && j0 + k < YL; ++k) orow[j0 + k] = w[k];
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) cur[k] = nxt[k];
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -536,11 +591,11 @@ int hr::filter_tc_execute_limited(const hr_filter_tc_plan* p, uint32_t* d_pairs,
   const size_t smem = (size_t)kStages * kStageBytes + 1024 + 128;
   HR_CUDA_TRY(cudaFuncSetAttribute(toeplitz_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long m_tiles = (p->rows + kBM - 1) / kBM;
-  const long long grid = m_tiles * p->n_tiles;
-  HR_REQUIRE(grid < (1LL << 31), "hr_filter_tc_execute: grid too large");
-  toeplitz_tc_kernel<<<(unsigned)grid, kThreads, smem, s>>>(p->m_a[0], p->m_a[1], p->m_a[2], p->m_t[0], p->m_t[1],
-                                                           p->m_t[2], d_pairs, p->rows, p->YL, p->n_tiles,
-                                                           p->KP / kBK, p->d_err, p->stall_kb, p->wait_limit);
+  const long long work = m_tiles * p->n_tiles;
+  const int grid = (int)std::min<long long>(work, hr::sm_count());  // persistent: one CTA per SM
+  toeplitz_tc_kernel<<<grid, kThreads, smem, s>>>(p->m_a[0], p->m_a[1], p->m_a[2], p->m_t[0], p->m_t[1], p->m_t[2],
+                                                  d_pairs, p->rows, p->YL, p->n_tiles, p->KP / kBK, work, p->d_err,
+                                                  p->stall_kb, p->wait_limit);
   HR_CUDA_TRY(cudaGetLastError());
   return HR_OK;
 }
