@@ -274,18 +274,40 @@ int hr::rebin_execute_limited(const hr_rebin_plan* p, float* d_out, const float*
 // Output view i reads the fan views FI - 1 and FI with FI = ceil((i DeltaTheta + beta_j) / DeltaFai) over the
 // channels j (clamped to the scan). Bounded here in double with one view of slack on each side for the float
 // rounding of the kernel's arithmetic.
-void hr::rebin_fan_views(const hr_rebin_plan* p, int i0, int i1, int* f0, int* f1) {
-  const double dt = p->DeltaTheta, df = p->DeltaFai;
+static void fan_view_bounds(double dt, double df, float beta_lo, float beta_hi, int ViewN, int i0, int i1, int* f0,
+                            int* f1) {
   double a = 1e300, b = -1e300;  // FaiIndex is monotone in i and in beta: its extremes are at the corners
   for (const int i : {i0, i1 - 1})
-    for (const float beta : {p->beta_lo, p->beta_hi}) {
+    for (const float beta : {beta_lo, beta_hi}) {
       const double x = (i * dt + beta) / df;
       a = std::min(a, x);
       b = std::max(b, x);
     }
   const double lo = std::floor(a) - 2.0, hi = std::ceil(b) + 1.0;
-  *f0 = (int)std::max(0.0, std::min(lo, (double)(p->ViewN - 1)));
-  *f1 = (int)std::max(0.0, std::min(hi, (double)(p->ViewN - 1)));
+  *f0 = (int)std::max(0.0, std::min(lo, (double)(ViewN - 1)));
+  *f1 = (int)std::max(0.0, std::min(hi, (double)(ViewN - 1)));
+}
+
+void hr::rebin_fan_views(const hr_rebin_plan* p, int i0, int i1, int* f0, int* f1) {
+  fan_view_bounds(p->DeltaTheta, p->DeltaFai, p->beta_lo, p->beta_hi, p->ViewN, i0, i1, f0, f1);
+}
+
+extern "C" int hr_rebin_fan_views(int YL, int ViewN, float YLC, float dYA, float DeltaTheta, float PLC, float DeltaT,
+                                  float DeltaFai, float SO, int i0, int i1, int* f0, int* f1) {
+  hr::clear_error();
+  HR_REQUIRE(f0 != nullptr && f1 != nullptr, "hr_rebin_fan_views: NULL argument");
+  HR_REQUIRE(YL > 0 && ViewN > 0 && DeltaFai != 0.0f && SO > 0.0f && dYA != 0.0f,
+             "hr_rebin_fan_views: invalid geometry");
+  HR_REQUIRE(0 <= i0 && i0 < i1 && i1 <= ViewN, "hr_rebin_fan_views: views [%d, %d) outside [0, %d)", i0, i1, ViewN);
+  std::vector<ChanInfo> tab;
+  channel_table(tab, YL, YLC, dYA, PLC, DeltaT, SO);
+  float lo = tab[0].beta, hi = tab[0].beta;
+  for (const ChanInfo& c : tab) {
+    lo = std::min(lo, c.beta);
+    hi = std::max(hi, c.beta);
+  }
+  fan_view_bounds(DeltaTheta, DeltaFai, lo, hi, ViewN, i0, i1, f0, f1);
+  return HR_OK;
 }
 
 extern "C" int hr_rebin_execute(const hr_rebin_plan* p, float* d_out, const float* d_proj, void* stream) {

@@ -135,6 +135,13 @@ int hr_rebin_plan_create(hr_rebin_plan** plan, int YL, int ZL, int ViewN, float 
 /* d_out, d_proj: device [ViewN][YL][ZL]. */
 int hr_rebin_execute(const hr_rebin_plan* plan, float* d_out, const float* d_proj, void* stream);
 void hr_rebin_plan_destroy(hr_rebin_plan* plan);
+/* Host only (no device needed): the fan views [*f0, *f1] that the rebinning of
+ * output views [i0, i1) reads (its bilinear taps over every channel, clamped to
+ * the scan, with a view or two of slack), for callers that stream the fan data
+ * in by ranges of views, as hr_recon_execute_host does. Same arguments as the
+ * rebinning (YLC, PLC 0-based). */
+int hr_rebin_fan_views(int YL, int ViewN, float YLC, float dYA, float DeltaTheta, float PLC, float DeltaT,
+                       float DeltaFai, float SO, int i0, int i1, int* f0, int* f1);
 
 /* ---- filter plan -------------------------------------------------------- */
 typedef struct hr_filter_plan hr_filter_plan;
