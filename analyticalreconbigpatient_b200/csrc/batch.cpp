@@ -402,38 +402,47 @@ extern "C" int hr_batch_execute_host(hr_batch_plan* p, float* const* h_vols, con
   for (int i = 0; i < p->n; ++i) dv[i] = p->d_hvol + p->voff[i];
   const bool fork = per_scan(p->variant);
   cudaStream_t s = p->sc;
-  for (int j = 0; j < p->n; ++j) {
-    const int i = order[j], b = j & 1;
-    // the fan of scan j goes to staging buffer b once scan j-2's rebinning has read it
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sin, p->consumed[b], 0));
-    HR_CUDA_TRY(cudaMemcpyAsync(p->d_stage[b], h_fans[i], fan_elems(p->d[i]) * sizeof(float),
-                                cudaMemcpyHostToDevice, p->sin));
-    HR_CUDA_TRY(cudaEventRecord(p->copied[b], p->sin));
-    HR_CUDA_TRY(cudaStreamWaitEvent(s, p->copied[b], 0));
-    HR_TRY(hr_rebin_execute(p->rebin[i], p->d_rebinned, p->d_stage[b], s));
-    HR_CUDA_TRY(cudaEventRecord(p->consumed[b], s));
-    HR_TRY(hr_filter_tc_execute(p->ftc[i], p->pairs[i], p->d_rebinned, HR_LAYOUT_REBIN, p->d[i].view0, s));
-    if (fork) {
-      // the scan's backprojection on its own stream, its volume out as soon as it is done
-      HR_TRY(fork_bp(p, i, dv[i], s));
-      HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->done[i], 0));
-      HR_CUDA_TRY(cudaMemcpyAsync(h_vols[i], dv[i], vol_elems(p->d[i]) * sizeof(float), cudaMemcpyDeviceToHost,
-                                  p->sout));
+  // Enqueues every scan; on a failure it returns with earlier work possibly in flight.
+  auto enqueue = [&]() -> int {
+    for (int j = 0; j < p->n; ++j) {
+      const int i = order[j], b = j & 1;
+      // the fan of scan j goes to staging buffer b once scan j-2's rebinning has read it
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sin, p->consumed[b], 0));
+      HR_CUDA_TRY(cudaMemcpyAsync(p->d_stage[b], h_fans[i], fan_elems(p->d[i]) * sizeof(float),
+                                  cudaMemcpyHostToDevice, p->sin));
+      HR_CUDA_TRY(cudaEventRecord(p->copied[b], p->sin));
+      HR_CUDA_TRY(cudaStreamWaitEvent(s, p->copied[b], 0));
+      HR_TRY(hr_rebin_execute(p->rebin[i], p->d_rebinned, p->d_stage[b], s));
+      HR_CUDA_TRY(cudaEventRecord(p->consumed[b], s));
+      HR_TRY(hr_filter_tc_execute(p->ftc[i], p->pairs[i], p->d_rebinned, HR_LAYOUT_REBIN, p->d[i].view0, s));
+      if (fork) {
+        // the scan's backprojection on its own stream, its volume out as soon as it is done
+        HR_TRY(fork_bp(p, i, dv[i], s));
+        HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->done[i], 0));
+        HR_CUDA_TRY(cudaMemcpyAsync(h_vols[i], dv[i], vol_elems(p->d[i]) * sizeof(float), cudaMemcpyDeviceToHost,
+                                    p->sout));
+      }
     }
+    if (!fork) {
+      HR_TRY(backproject(p, dv.data(), p->variant, s));
+      HR_CUDA_TRY(cudaEventRecord(p->bp_done, s));
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->bp_done, 0));
+      for (int i = 0; i < p->n; ++i)
+        HR_CUDA_TRY(cudaMemcpyAsync(h_vols[i], dv[i], vol_elems(p->d[i]) * sizeof(float), cudaMemcpyDeviceToHost,
+                                    p->sout));
+    } else {
+      HR_TRY(join_all(p, s));
+    }
+    return HR_OK;
+  };
+  int st = enqueue();
+  // whether or not everything was enqueued, no copy may still use the caller's buffers on return
+  for (cudaStream_t s2 : {p->sout, s, p->sin}) {
+    const cudaError_t e = cudaStreamSynchronize(s2);
+    if (e != cudaSuccess && st == HR_OK)
+      st = hr::fail(HR_ERR_CUDA, "hr_batch_execute_host: %s", cudaGetErrorString(e));
   }
-  if (!fork) {
-    HR_TRY(backproject(p, dv.data(), p->variant, s));
-    HR_CUDA_TRY(cudaEventRecord(p->bp_done, s));
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->bp_done, 0));
-    for (int i = 0; i < p->n; ++i)
-      HR_CUDA_TRY(cudaMemcpyAsync(h_vols[i], dv[i], vol_elems(p->d[i]) * sizeof(float), cudaMemcpyDeviceToHost,
-                                  p->sout));
-  } else {
-    HR_TRY(join_all(p, s));
-  }
-  HR_CUDA_TRY(cudaStreamSynchronize(p->sout));
-  HR_CUDA_TRY(cudaStreamSynchronize(s));
-  HR_CUDA_TRY(cudaStreamSynchronize(p->sin));
+  HR_TRY(st);
   return hr_batch_check(p);
 }
 

@@ -456,11 +456,13 @@ __global__ void tex_fill_kernel(float* __restrict__ scale, const unsigned long l
     if (blockIdx.x == 0 && threadIdx.x == 0) scale[0] = 1.0f;
   }
   const int lmask = (1 << lsh) - 1;
-  if (HALF && (YL & 3) == 0) {
-    // four channels per thread: one 16-byte load of their pairs, one 8-byte (four-texel) surface store
+  if (HALF && (YL & 3) == 0 && (reinterpret_cast<uintptr_t>(fpb) & 15) == 0) {
+    // four channels per thread: one 16-byte load of their pairs (rows start 16-byte aligned), one 8-byte
+    // (four-texel) surface store
     const int G = YL >> 2;
     const long long n = (r1 - r0) * G;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
       const long long r = r0 + i / G;
       const int g = (int)(i - (r - r0) * G);
       const int p = (int)(r / ZL), v = (int)(r - (long long)p * ZL);

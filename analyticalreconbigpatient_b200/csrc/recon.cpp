@@ -258,53 +258,64 @@ int execute_host_streamed(hr_recon_plan* p, float* h_vol, const float* h_fan, bo
   const bool tex = f->tex.kind != 0;
   const size_t per_view = (size_t)d.YL * d.ZL;
   const int ctas = 8 * hr::sm_count();  // rebin and split CTAs beside a running backprojection
-  // everything before this call on the plan's own stream comes first
-  HR_CUDA_TRY(cudaEventRecord(p->ev_in[0], p->stream));
-  for (cudaStream_t st : {p->sf, p->sbp, p->scopy, p->sout}) HR_CUDA_TRY(cudaStreamWaitEvent(st, p->ev_in[0], 0));
-  int copied = 0, filled = -1;
-  size_t r = 0;
-  for (int c = 0; c < nch; ++c) {
-    const int p0 = c * C, p1 = std::min(PN, p0 + C);
-    int f0 = 0, f1 = 0;
-    hr::rebin_fan_views(p->rebin, d.view0 + p0, d.view0 + p1, &f0, &f1);
-    if (c == nch - 1) f1 = d.ViewN - 1;
-    if (f1 + 1 > copied) {
-      HR_CUDA_TRY(cudaMemcpyAsync(p->d_fan + copied * per_view, h_fan + copied * per_view,
-                                  (size_t)(f1 + 1 - copied) * per_view * sizeof(float), cudaMemcpyDefault,
-                                  p->scopy));
-      copied = f1 + 1;
-    }
-    HR_CUDA_TRY(cudaEventRecord(p->ev_in[c], p->scopy));
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sf, p->ev_in[c], 0));
-    HR_TRY(hr::rebin_execute_range(p->rebin, p->d_rebinned, p->d_fan, d.view0 + p0, d.view0 + p1, ctas, p->sf));
-    HR_TRY(hr::filter_tc_execute_limited(p->fchunk[p1 - p0 == C ? 0 : 1], p->d_pairs + p0 * per_view,
-                                         p->d_rebinned, HR_LAYOUT_REBIN, d.view0 + p0, ctas, p->sf));
-    HR_CUDA_TRY(cudaEventRecord(p->ev_filt[c], p->sf));
-    // backprojection ranges whose windows this chunk completes: fill the chunks they need, then launch
-    for (; r < ranges.size() && ranges[r].ready <= c; ++r) {
-      for (; filled < ranges[r].ready; ++filled) {
-        const int q = filled + 1;
-        HR_CUDA_TRY(cudaStreamWaitEvent(p->sbp, p->ev_filt[q], 0));
-        if (tex)
-          HR_TRY(hr::bp_fast_tex_fill_range(*f, *g, p->d_pairs, q * C, std::min(PN, (q + 1) * C), q == 0 ? 1 : 2,
-                                            p->sbp));
+  // Enqueues the copies and kernels; on a failure it returns with earlier work possibly in flight.
+  auto enqueue = [&]() -> int {
+    // everything before this call on the plan's own stream comes first
+    HR_CUDA_TRY(cudaEventRecord(p->ev_in[0], p->stream));
+    for (cudaStream_t st : {p->sf, p->sbp, p->scopy, p->sout}) HR_CUDA_TRY(cudaStreamWaitEvent(st, p->ev_in[0], 0));
+    int copied = 0, filled = -1;
+    size_t r = 0;
+    for (int c = 0; c < nch; ++c) {
+      const int p0 = c * C, p1 = std::min(PN, p0 + C);
+      int f0 = 0, f1 = 0;
+      hr::rebin_fan_views(p->rebin, d.view0 + p0, d.view0 + p1, &f0, &f1);
+      if (c == nch - 1) f1 = d.ViewN - 1;
+      if (f1 + 1 > copied) {
+        HR_CUDA_TRY(cudaMemcpyAsync(p->d_fan + copied * per_view, h_fan + copied * per_view,
+                                    (size_t)(f1 + 1 - copied) * per_view * sizeof(float), cudaMemcpyDefault,
+                                    p->scopy));
+        copied = f1 + 1;
       }
-      HR_TRY(hr::bp_fast_execute_blocks(*f, *g, p->d_vol, p->d_pairs, ranges[r].b0, ranges[r].b1 - ranges[r].b0,
-                                        p->sbp));
-      HR_CUDA_TRY(cudaEventRecord(p->ev_bp[r], p->sbp));
+      HR_CUDA_TRY(cudaEventRecord(p->ev_in[c], p->scopy));
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sf, p->ev_in[c], 0));
+      HR_TRY(hr::rebin_execute_range(p->rebin, p->d_rebinned, p->d_fan, d.view0 + p0, d.view0 + p1, ctas, p->sf));
+      HR_TRY(hr::filter_tc_execute_limited(p->fchunk[p1 - p0 == C ? 0 : 1], p->d_pairs + p0 * per_view,
+                                           p->d_rebinned, HR_LAYOUT_REBIN, d.view0 + p0, ctas, p->sf));
+      HR_CUDA_TRY(cudaEventRecord(p->ev_filt[c], p->sf));
+      // backprojection ranges whose windows this chunk completes: fill the chunks they need, then launch
+      for (; r < ranges.size() && ranges[r].ready <= c; ++r) {
+        for (; filled < ranges[r].ready; ++filled) {
+          const int q = filled + 1;
+          HR_CUDA_TRY(cudaStreamWaitEvent(p->sbp, p->ev_filt[q], 0));
+          if (tex)
+            HR_TRY(hr::bp_fast_tex_fill_range(*f, *g, p->d_pairs, q * C, std::min(PN, (q + 1) * C), q == 0 ? 1 : 2,
+                                              p->sbp));
+        }
+        HR_TRY(hr::bp_fast_execute_blocks(*f, *g, p->d_vol, p->d_pairs, ranges[r].b0, ranges[r].b1 - ranges[r].b0,
+                                          p->sbp));
+        HR_CUDA_TRY(cudaEventRecord(p->ev_bp[r], p->sbp));
+      }
     }
+    // volume out, range by range (enqueued last: a copy to pageable memory returns only when it is done); the
+    // copies take their direction from the addresses, so h_vol (and h_fan) may also be device memory
+    const size_t ld = (size_t)d.bp.ZN * sizeof(float);
+    for (size_t j = 0; j < ranges.size(); ++j) {
+      const int z0 = ranges[j].b0 * t.nz, z1 = std::min(d.bp.ZN, ranges[j].b1 * t.nz);
+      if (z1 <= z0) continue;
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->ev_bp[j], 0));
+      HR_CUDA_TRY(cudaMemcpy2DAsync(h_vol + z0, ld, p->d_vol + z0, ld, (size_t)(z1 - z0) * sizeof(float),
+                                    (size_t)d.bp.XN * d.bp.YN, cudaMemcpyDefault, p->sout));
+    }
+    return HR_OK;
+  };
+  int st = enqueue();
+  // whether or not everything was enqueued, no copy may still read or write the caller's buffers on return
+  for (cudaStream_t s2 : {p->scopy, p->sf, p->sbp, p->sout}) {
+    const cudaError_t e = cudaStreamSynchronize(s2);
+    if (e != cudaSuccess && st == HR_OK)
+      st = hr::fail(HR_ERR_CUDA, "hr_recon_execute_host: %s", cudaGetErrorString(e));
   }
-  // volume out, range by range (enqueued last: a copy to pageable memory returns only when it is done); the
-  // copies take their direction from the addresses, so h_vol (and h_fan) may also be device memory
-  const size_t ld = (size_t)d.bp.ZN * sizeof(float);
-  for (size_t j = 0; j < ranges.size(); ++j) {
-    const int z0 = ranges[j].b0 * t.nz, z1 = std::min(d.bp.ZN, ranges[j].b1 * t.nz);
-    if (z1 <= z0) continue;
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->ev_bp[j], 0));
-    HR_CUDA_TRY(cudaMemcpy2DAsync(h_vol + z0, ld, p->d_vol + z0, ld, (size_t)(z1 - z0) * sizeof(float),
-                                  (size_t)d.bp.XN * d.bp.YN, cudaMemcpyDefault, p->sout));
-  }
-  for (cudaStream_t st : {p->scopy, p->sf, p->sbp, p->sout}) HR_CUDA_TRY(cudaStreamSynchronize(st));
+  HR_TRY(st);
   *done = true;
   for (hr_filter_tc_plan* fc : p->fchunk)
     if (fc) HR_TRY(hr_filter_tc_check(fc));
@@ -333,10 +344,17 @@ extern "C" int hr_recon_execute_host(hr_recon_plan* p, float* h_vol, const float
   }
   const size_t nfan = (size_t)p->d.YL * p->d.ZL * p->d.ViewN;
   const size_t nvol = (size_t)p->d.bp.XN * p->d.bp.YN * p->d.bp.ZN;
-  HR_CUDA_TRY(cudaMemcpyAsync(p->d_fan, h_fan, nfan * sizeof(float), cudaMemcpyDefault, p->stream));
-  HR_TRY(hr_recon_execute(p, p->d_vol, p->d_fan, p->stream));
-  HR_CUDA_TRY(cudaMemcpyAsync(h_vol, p->d_vol, nvol * sizeof(float), cudaMemcpyDefault, p->stream));
-  HR_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  auto enqueue = [&]() -> int {
+    HR_CUDA_TRY(cudaMemcpyAsync(p->d_fan, h_fan, nfan * sizeof(float), cudaMemcpyDefault, p->stream));
+    HR_TRY(hr_recon_execute(p, p->d_vol, p->d_fan, p->stream));
+    HR_CUDA_TRY(cudaMemcpyAsync(h_vol, p->d_vol, nvol * sizeof(float), cudaMemcpyDefault, p->stream));
+    return HR_OK;
+  };
+  const int st = enqueue();
+  // no copy may still read or write the caller's buffers on return, also after a failure
+  const cudaError_t e = cudaStreamSynchronize(p->stream);
+  HR_TRY(st);
+  HR_CUDA_TRY(e);
   return HR_OK;
 }
 

@@ -393,37 +393,44 @@ extern "C" int hr_slab_execute_range(hr_slab_plan* p, float* vol, const float* f
   const hr_bp_geom& G = p->d.bp;
   const SlabLayout& L = p->L;
   const int n = (int)p->mine.size();
-  HR_TRY(enqueue_fan_copy(p, 0, fan, fan_view0, fan_on_host != 0, true));
-  for (int j = 0; j < n; ++j) {
-    const int k = p->mine[j], b = j & 1;
-    // rebin + filter of slab j on the filter stream (under slab j-1's backprojection)
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sf, p->copied[b], 0));
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sf, p->computed[b], 0));  // slab j-2's backprojection has read d_pairs[b]
-    HR_CUDA_TRY(cudaGraphLaunch(p->gfilter[b], p->sf));
-    HR_CUDA_TRY(cudaEventRecord(p->consumed[b], p->sf));
-    HR_CUDA_TRY(cudaEventRecord(p->filtered[b], p->sf));
-    if (j + 1 < n) HR_TRY(enqueue_fan_copy(p, j + 1, fan, fan_view0, fan_on_host != 0, true));
-    // tables of slab k: host build (overlaps the GPU), stream-ordered upload, backprojection
-    hr::BpFastHost h;
-    HR_TRY(hr::bp_fast_host_tables(&h, slab_geom(p, k), p->w.data()));
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->filtered[b], 0));
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->drained[b], 0));  // slab j-2's volume has left d_vslab[b]
-    HR_TRY(hr::bp_fast_upload(&p->fast[b], h, p->sc));
-    HR_CUDA_TRY(cudaGraphLaunch(p->gbp[b], p->sc));
-    HR_CUDA_TRY(cudaEventRecord(p->computed[b], p->sc));
-    // the slab's slices are a strided block of the z-fastest volume; copied out
-    // on the output stream while the next slab computes
-    const size_t ld = (size_t)G.ZN * 4;
-    HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->computed[b], 0));
-    HR_CUDA_TRY(cudaMemcpy2DAsync(vol + L.first_slice[k], ld, p->d_vslab[b], (size_t)L.S * 4,
-                                  (size_t)L.n_slices[k] * 4, (size_t)G.XN * G.YN,
-                                  vol_on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, p->sout));
-    HR_CUDA_TRY(cudaEventRecord(p->drained[b], p->sout));
+  // Enqueues every slab; on a failure it returns with earlier work possibly in flight.
+  auto enqueue = [&]() -> int {
+    HR_TRY(enqueue_fan_copy(p, 0, fan, fan_view0, fan_on_host != 0, true));
+    for (int j = 0; j < n; ++j) {
+      const int k = p->mine[j], b = j & 1;
+      // rebin + filter of slab j on the filter stream (under slab j-1's backprojection)
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sf, p->copied[b], 0));
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sf, p->computed[b], 0));  // slab j-2's backprojection has read d_pairs[b]
+      HR_CUDA_TRY(cudaGraphLaunch(p->gfilter[b], p->sf));
+      HR_CUDA_TRY(cudaEventRecord(p->consumed[b], p->sf));
+      HR_CUDA_TRY(cudaEventRecord(p->filtered[b], p->sf));
+      if (j + 1 < n) HR_TRY(enqueue_fan_copy(p, j + 1, fan, fan_view0, fan_on_host != 0, true));
+      // tables of slab k: host build (overlaps the GPU), stream-ordered upload, backprojection
+      hr::BpFastHost h;
+      HR_TRY(hr::bp_fast_host_tables(&h, slab_geom(p, k), p->w.data()));
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->filtered[b], 0));
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sc, p->drained[b], 0));  // slab j-2's volume has left d_vslab[b]
+      HR_TRY(hr::bp_fast_upload(&p->fast[b], h, p->sc));
+      HR_CUDA_TRY(cudaGraphLaunch(p->gbp[b], p->sc));
+      HR_CUDA_TRY(cudaEventRecord(p->computed[b], p->sc));
+      // the slab's slices are a strided block of the z-fastest volume; copied out
+      // on the output stream while the next slab computes
+      const size_t ld = (size_t)G.ZN * 4;
+      HR_CUDA_TRY(cudaStreamWaitEvent(p->sout, p->computed[b], 0));
+      HR_CUDA_TRY(cudaMemcpy2DAsync(vol + L.first_slice[k], ld, p->d_vslab[b], (size_t)L.S * 4,
+                                    (size_t)L.n_slices[k] * 4, (size_t)G.XN * G.YN,
+                                    vol_on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, p->sout));
+      HR_CUDA_TRY(cudaEventRecord(p->drained[b], p->sout));
+    }
+    return HR_OK;
+  };
+  int st = enqueue();
+  // whether or not everything was enqueued, no copy may still use the caller's buffers on return
+  for (cudaStream_t s2 : {p->sout, p->sc, p->sf, p->scopy}) {
+    const cudaError_t e = cudaStreamSynchronize(s2);
+    if (e != cudaSuccess && st == HR_OK) st = hr::fail(HR_ERR_CUDA, "hr_slab_execute: %s", cudaGetErrorString(e));
   }
-  HR_CUDA_TRY(cudaStreamSynchronize(p->sout));
-  HR_CUDA_TRY(cudaStreamSynchronize(p->sc));
-  HR_CUDA_TRY(cudaStreamSynchronize(p->sf));
-  HR_CUDA_TRY(cudaStreamSynchronize(p->scopy));
+  HR_TRY(st);
   return hr_filter_tc_check(p->ftc);
 }
 
