@@ -107,6 +107,7 @@ _SIGS = {
     "hr_slab_plan_destroy": (None, [_p]),
     "hr_slab_windows": (_i, [ctypes.POINTER(ReconDesc), _i, _i, _i, _i, _p, _i, ctypes.POINTER(_i)]),
     "hr_rebin_fan_views": (_i, [_i, _i] + [_f] * 7 + [_i, _i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "hr_recon_stream_schedule": (_i, [ctypes.POINTER(ReconDesc), _i, _i, _p, _i, ctypes.POINTER(_i)]),
     "hr_slab_plan_create_part": (_i, [ctypes.POINTER(_p), ctypes.POINTER(ReconDesc), _i, _i, _i, _i]),
     "hr_slab_execute_range": (_i, [_p, _p, _p, _i, _i, _i]),
     "hr_slab_fan_range": (_i, [_p, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_size_t)]),

@@ -366,7 +366,8 @@ constexpr int kNzFp64 = 4;
 // Checks a backprojection geometry and fills the kernels' parameter block. Every
 // entry that backprojects (the plans and the allocation-free entry) goes through
 // it, so they accept exactly the same geometries.
-int bp_params_from_geom(const hr_bp_geom* g, const char* who, BpParams* out) {
+// The geometry checks of every backprojection entry (host only); *half: the window's half width.
+int geom_checks(const hr_bp_geom* g, const char* who, int* half_out) {
   HR_REQUIRE(g->XN > 0 && g->YN > 0 && g->ZN > 0 && g->YL > 1 && g->ZL > 1 && g->PN > 0 && g->N_2pi > 1,
              "%s: invalid sizes", who);
   HR_REQUIRE(g->h != 0.0 && g->DeltaFai != 0.0 && g->dYL != 0.0 && g->dZL != 0.0 && g->SO > 0.0,
@@ -380,6 +381,13 @@ int bp_params_from_geom(const hr_bp_geom* g, const char* who, BpParams* out) {
   HR_REQUIRE(half >= 0 && (double)half <= g->N_pi && g->N_pi + half <= g->N_2pi - 1 &&
                  2.0 * g->N_pi <= g->N_2pi + 1e-9,
              "%s: HSCoef=%g, N_pi=%g give a view window outside the weight table", who, g->HSCoef, g->N_pi);
+  *half_out = half;
+  return HR_OK;
+}
+
+int bp_params_from_geom(const hr_bp_geom* g, const char* who, BpParams* out) {
+  int half = 0;
+  HR_TRY(geom_checks(g, who, &half));
   HR_TRY(hr::require_device());
   BpParams P{};
   P.XN = g->XN; P.YN = g->YN; P.ZN = g->ZN; P.YL = g->YL; P.ZL = g->ZL; P.PN = g->PN; P.N_2pi = g->N_2pi;
@@ -452,6 +460,21 @@ void fill_view_table(ViewTab* tab, int PN, double BetaS, double DeltaFai, double
 
 }  // namespace
 
+void hr::fast_geom_fill(const hr_bp_geom& g, int half, BpFastGeom* f) {
+  f->XN = g.XN; f->YN = g.YN; f->ZN = g.ZN; f->YL = g.YL; f->ZL = g.ZL; f->PN = g.PN; f->half = half;
+  f->XNC = g.XNC; f->YNC = g.YNC; f->ZNC = g.ZNC; f->dx = g.dx; f->dy = g.dy; f->dz = g.dz;
+  f->YLC = g.YLC; f->ZLC = g.ZLC; f->dYL = g.dYL; f->dZL = g.dZL; f->h = g.h; f->BetaS = g.BetaS;
+  f->DeltaFai = g.DeltaFai; f->N_pi = g.N_pi; f->SO = g.SO; f->SD = g.SD; f->k1 = g.k1;
+  f->ZN_valid = g.ZN;
+}
+
+int hr::fast_geom_of(const hr_bp_geom& g, BpFastGeom* f) {
+  int half = 0;
+  HR_TRY(geom_checks(&g, "backprojection", &half));
+  fast_geom_fill(g, half, f);
+  return HR_OK;
+}
+
 extern "C" int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const double* w, int form) {
   hr::clear_error();
   HR_REQUIRE(plan != nullptr && g != nullptr && w != nullptr, "hr_bp_plan_create: NULL argument");
@@ -469,13 +492,8 @@ extern "C" int hr_bp_plan_create(hr_bp_plan** plan, const hr_bp_geom* g, const d
 
   hr_bp_plan* pl = new hr_bp_plan{P, form, nullptr, nullptr, nullptr, hr::BpFastGeom{}, hr::BpFast{}};
   if (form == HR_FORM_FAST) {
-    hr::BpFastGeom& f = pl->fg;
-    f.XN = g->XN; f.YN = g->YN; f.ZN = g->ZN; f.YL = g->YL; f.ZL = g->ZL; f.PN = g->PN; f.half = half;
-    f.XNC = g->XNC; f.YNC = g->YNC; f.ZNC = g->ZNC; f.dx = g->dx; f.dy = g->dy; f.dz = g->dz;
-    f.YLC = g->YLC; f.ZLC = g->ZLC; f.dYL = g->dYL; f.dZL = g->dZL; f.h = g->h; f.BetaS = g->BetaS;
-    f.DeltaFai = g->DeltaFai; f.N_pi = g->N_pi; f.SO = g->SO; f.SD = g->SD; f.k1 = g->k1;
-    f.ZN_valid = g->ZN;
-    const int st = hr::bp_fast_create(&pl->fast, f, w);
+    hr::fast_geom_fill(*g, half, &pl->fg);
+    const int st = hr::bp_fast_create(&pl->fast, pl->fg, w);
     if (st != HR_OK) {
       hr::bp_fast_destroy(&pl->fast);
       delete pl;

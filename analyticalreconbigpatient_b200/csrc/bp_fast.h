@@ -7,6 +7,8 @@
 #include <cstdint>
 #include <vector>
 
+#include "helixrecon.h"
+
 struct hr_bp_plan;
 
 namespace hr {
@@ -192,6 +194,9 @@ int bp_fast_best_tex_variant(const BpFast& f);
 int bp_fast_variant_nz(int v);
 // The fast-form geometry and tables of a backprojection plan (HR_FORM_FAST).
 int bp_plan_fast_parts(const hr_bp_plan* plan, const BpFastGeom** g, const BpFast** f);
+// The fast-form geometry of a backprojection geometry (checked as hr_bp_plan_create checks it), host only.
+int fast_geom_of(const hr_bp_geom& g, BpFastGeom* f);
+void fast_geom_fill(const hr_bp_geom& g, int half, BpFastGeom* f);
 // FP32 rows [rows][YL] -> BF16 channel pairs: word u = bf16(x[u]) | bf16(x[u+1]) << 16.
 int pack_pairs(uint32_t* out, const float* in, long long rows, int YL, cudaStream_t s);
 

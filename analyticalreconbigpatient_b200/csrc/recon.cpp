@@ -334,6 +334,32 @@ int execute_host_streamed(hr_recon_plan* p, float* h_vol, const float* h_fan, bo
 
 }  // namespace
 
+extern "C" int hr_recon_stream_schedule(const hr_recon_desc* d, int nz, int chunk, int* out, int cap, int* n) {
+  hr::clear_error();
+  HR_REQUIRE(d != nullptr && d->w != nullptr && n != nullptr, "hr_recon_stream_schedule: NULL argument");
+  HR_REQUIRE(chunk > 0, "hr_recon_stream_schedule: chunk of %d views", chunk);
+  int set = -1;
+  for (int i = 0; i < hr::kFastTableSets; ++i)
+    if (hr::kFastNz[i] == nz) set = i;
+  HR_REQUIRE(set >= 0, "hr_recon_stream_schedule: %d slices per z block (16, 8 or 4)", nz);
+  hr::BpFastGeom g;
+  HR_TRY(hr::fast_geom_of(d->bp, &g));
+  hr::BpFastHost h;  // the tables a fast backprojection plan builds, on the host
+  HR_TRY(hr::bp_fast_host_tables(&h, g, d->w));
+  const hr::BpFastHostSet& t = h.set[set];
+  const std::vector<int> zb(t.zb.begin(), t.zb.begin() + 2 * (size_t)t.nblocks);
+  const std::vector<BpRange> r = bp_ranges(zb, t.nblocks, std::min(chunk, d->bp.PN), d->bp.PN);
+  *n = (int)r.size();
+  if (out == nullptr) return HR_OK;
+  HR_REQUIRE(cap >= (int)r.size(), "hr_recon_stream_schedule: %d ranges, room for %d", (int)r.size(), cap);
+  for (size_t j = 0; j < r.size(); ++j) {
+    out[3 * j] = r[j].b0;
+    out[3 * j + 1] = r[j].b1;
+    out[3 * j + 2] = r[j].ready;
+  }
+  return HR_OK;
+}
+
 extern "C" int hr_recon_execute_host(hr_recon_plan* p, float* h_vol, const float* h_fan) {
   hr::clear_error();
   HR_REQUIRE(p != nullptr && h_vol != nullptr && h_fan != nullptr, "hr_recon_execute_host: NULL argument");

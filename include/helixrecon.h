@@ -281,6 +281,14 @@ int hr_recon_execute(const hr_recon_plan* plan, float* d_vol, const float* d_fan
  * equals the device entry's to FP32 rounding, and is refilled whole (the
  * device entry's bits) when a later chunk exceeds that scale. */
 int hr_recon_execute_host(hr_recon_plan* plan, float* h_vol, const float* h_fan);
+/* Host only (no device needed): the backprojection ranges of the streamed host
+ * execution for a scan, with nz slices per z block (the chosen variant's: 16,
+ * 8 or 4) and chunks of `chunk` parallel views: *n ranges, written to out as
+ * {first z block, end z block, chunk after whose filtering the range may run}
+ * (out may be NULL to count them; cap: triples out holds). Zero ranges: the
+ * scan's view windows do not complete in z order, and the host execution runs
+ * the chain unstreamed. */
+int hr_recon_stream_schedule(const hr_recon_desc* desc, int nz, int chunk, int* out, int cap, int* n);
 /* One-line description of the plan's kernel configuration (the fast form's
  * backprojection is autotuned at plan creation). */
 int hr_recon_describe(const hr_recon_plan* plan, char* buf, int len);
